@@ -1,0 +1,143 @@
+"""ctypes binding of ``libnrldpc_b200.so`` (the C ABI in include/nrldpc_b200.h).
+
+The record classes mirror the reference's ctypes structs
+(scripts/ldpc_c_sim_common.py:32-57, deep_learning/ldpc_table_config.py:19-54)
+field for field, so either set of classes can be passed to either library.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libnrldpc_b200.so")
+
+NRLDPC_OK = 0
+NRLDPC_NOT_CONVERGED = 1
+NRLDPC_ERR_CUDA = -1
+NRLDPC_ERR_CONFIG = -2
+NRLDPC_ERR_ALGO = -3
+NRLDPC_ERR_ARG = -4
+
+BG_ROWS = {1: 46, 2: 42}
+BG_COLS = {1: 68, 2: 52}
+BG_NNZ = {1: 316, 2: 197}
+
+
+class LdpcInConfig(ctypes.Structure):
+    """ldpc_in_config_t: seven uint16_t (c_lib/nr_ldpc.h:42-50)."""
+
+    _fields_ = [(n, ctypes.c_uint16) for n in ("bgn", "A", "crctype", "E", "rv", "Qm", "HARQ_on")]
+
+
+class DecoderConfig(ctypes.Structure):
+    """ldpc_decoder_cfg_t (c_lib/nr_ldpc.h:82-90)."""
+
+    _fields_ = [
+        ("algo", ctypes.c_uint16),
+        ("max_iterations", ctypes.c_uint16),
+        ("alpha", ctypes.c_uint16),
+        ("beta", ctypes.c_uint16),
+        ("filling_bit_value", ctypes.c_int16),
+        ("max_llr", ctypes.c_int16),
+        ("min_llr", ctypes.c_int16),
+    ]
+
+
+class LdpcConfig(ctypes.Structure):
+    """ldpc_config_t (c_lib/nr_ldpc.h:54-79)."""
+
+    _fields_ = [(n, ctypes.c_uint16) for n in (
+        "bgn", "A", "crctype", "E", "rv", "Qm", "HARQ_on", "B", "Zc", "iLS", "K", "F", "N", "k0")] + [
+        ("Vij_array", ctypes.POINTER(ctypes.c_uint16)),
+        ("HBG_array", ctypes.POINTER(ctypes.c_uint16)),
+        ("HBG_offset_array", ctypes.POINTER(ctypes.c_uint16)),
+    ]
+
+
+def make_decoder_config(values) -> DecoderConfig:
+    """Row [algo, max_iterations, alpha, beta, filling_bit_value, max_llr, min_llr]
+    (scripts/ldpc_c_sim_common.py:112-122)."""
+    return DecoderConfig(*[int(v) for v in values])
+
+
+def make_in_config(bgn, A, crctype, E, rv=0, Qm=2, HARQ_on=0) -> LdpcInConfig:
+    return LdpcInConfig(bgn, A, crctype, E, rv, Qm, HARQ_on)
+
+
+_lock = threading.Lock()
+_lib = None
+
+EXPORTED_SYMBOLS = (
+    "gen_ldpc_parameters",
+    "cuda_ldpc_5g_decode",
+    "c_ldpc_5g_decode",
+    "calculate_crc",
+    "nrldpc_decode_batch",
+    "nrldpc_decode_batch_host",
+    "nrldpc_set_trained_weights",
+    "nrldpc_set_degree_alpha",
+    "nrldpc_kernel_launch_count",
+    "nrldpc_version",
+)
+
+
+def load_library(path: str | None = None) -> ctypes.CDLL:
+    """Load the CUDA library (building it first if it is missing and nvcc exists).
+
+    Raises if the library cannot be found or built: there is no CPU fallback.
+    """
+    global _lib
+    with _lock:
+        if _lib is not None and path is None:
+            return _lib
+        p = path or LIB_PATH
+        if not os.path.exists(p):
+            from .build import build_library
+
+            p = build_library()
+        lib = ctypes.CDLL(p)
+        _declare(lib)
+        if path is None:
+            _lib = lib
+        return lib
+
+
+def _declare(lib: ctypes.CDLL) -> None:
+    vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32
+    lib.gen_ldpc_parameters.argtypes = [ctypes.POINTER(LdpcConfig), ctypes.POINTER(LdpcInConfig)]
+    lib.gen_ldpc_parameters.restype = ctypes.c_int
+    for name in ("cuda_ldpc_5g_decode", "c_ldpc_5g_decode"):
+        f = getattr(lib, name)
+        f.argtypes = [vp, vp, ctypes.POINTER(LdpcInConfig), ctypes.POINTER(DecoderConfig)]
+        f.restype = i32
+    lib.calculate_crc.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.calculate_crc.restype = ctypes.c_uint32
+    lib.nrldpc_decode_batch.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig), ctypes.POINTER(DecoderConfig),
+                                        vp, i64, vp, vp, vp, i64, vp, i64, vp]
+    lib.nrldpc_decode_batch.restype = i32
+    lib.nrldpc_decode_batch_host.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig),
+                                             ctypes.POINTER(DecoderConfig), vp, i64, vp, vp, vp]
+    lib.nrldpc_decode_batch_host.restype = i32
+    lib.nrldpc_set_trained_weights.argtypes = [ctypes.c_uint16, vp, vp, i32]
+    lib.nrldpc_set_trained_weights.restype = i32
+    lib.nrldpc_set_degree_alpha.argtypes = [vp]
+    lib.nrldpc_set_degree_alpha.restype = i32
+    lib.nrldpc_kernel_launch_count.argtypes = []
+    lib.nrldpc_kernel_launch_count.restype = i64
+    lib.nrldpc_version.argtypes = []
+    lib.nrldpc_version.restype = ctypes.c_char_p
+
+
+def gen_ldpc_parameters(cfg: LdpcInConfig, lib=None) -> LdpcConfig:
+    lib = lib or load_library()
+    out = LdpcConfig()
+    if lib.gen_ldpc_parameters(ctypes.byref(out), ctypes.byref(cfg)) != 0:
+        raise ValueError("invalid LDPC configuration")
+    return out
+
+
+def kernel_launch_count(lib=None) -> int:
+    return int((lib or load_library()).nrldpc_kernel_launch_count())

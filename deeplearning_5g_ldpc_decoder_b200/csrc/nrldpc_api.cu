@@ -1,0 +1,496 @@
+// nrldpc_api.cu — the C ABI: reference-compatible entry points and the
+// batched device API.  Host code only; kernels live in nrldpc_fixed.cu and
+// nrldpc_float.cu.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <utility>
+#include <vector>
+
+#include "nrldpc_internal.h"
+
+namespace nrldpc {
+
+namespace {
+
+std::atomic<int64_t> g_launches{0};
+std::mutex g_mu;
+
+// Default algo-3 table: alpha by check-node degree
+// (c_lib/degree_fixedpoint_ldpc_decoder.c:188-222).
+const int16_t kDefaultDegreeAlpha[kMaxDegree] = {26623, 26623, 26623, 26623, 24575, 24575, 24575,
+                                                 24575, 22527, 22527, 22527, 22527, 22527, 22527,
+                                                 22527, 22527, 22527, 22527, 22527};
+int16_t g_degree_alpha[kMaxDegree];
+bool g_degree_alpha_init = false;
+
+int16_t degree_alpha(int deg) {
+  if (!g_degree_alpha_init) {
+    memcpy(g_degree_alpha, kDefaultDegreeAlpha, sizeof(g_degree_alpha));
+    g_degree_alpha_init = true;
+  }
+  if (deg <= 0) return g_degree_alpha[0];
+  if (deg > kMaxDegree) return g_degree_alpha[kMaxDegree - 1];
+  return g_degree_alpha[deg - 1];
+}
+
+// Algo-2 tables, [T][rows] packed alpha|beta<<16.  The built-in table is
+// what the reference compiles in today (c_lib/BG1_trained_ldpc_weights.c:25-33,
+// BG2_trained_ldpc_weights.c): for 32 iterations, alpha by the row-degree
+// rule (26623 for degree <= 4, 24575 for 5..8, 22527 above) and beta 0.
+struct TrainedTable {
+  std::vector<uint32_t> ab;
+  int T = 0;
+  uint64_t generation = 0;
+};
+TrainedTable g_trained[2];
+uint64_t g_trained_gen = 1;
+
+void default_trained(int bgn, TrainedTable* t) {
+  const BaseGraph& g = base_graph(bgn);
+  t->T = 32;
+  t->ab.assign((size_t)t->T * g.rows, 0u);
+  for (int it = 0; it < t->T; ++it) {
+    for (int r = 0; r < g.rows; ++r) {
+      const int d = g.degree[r];
+      const int16_t a = d <= 4 ? 26623 : (d <= 8 ? 24575 : 22527);
+      t->ab[(size_t)it * g.rows + r] = pack_ab(a, 0);
+    }
+  }
+  t->generation = g_trained_gen++;
+}
+
+TrainedTable& trained(int bgn) {
+  TrainedTable& t = g_trained[bgn == 1 ? 0 : 1];
+  if (t.T == 0) default_trained(bgn, &t);
+  return t;
+}
+
+struct Buffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+int ensure(Buffer* b, size_t bytes) {
+  if (b->bytes >= bytes && b->ptr) return 0;
+  if (b->ptr) cudaFree(b->ptr);
+  b->ptr = nullptr;
+  b->bytes = 0;
+  size_t want = std::max(bytes, (size_t)256);
+  cudaError_t e = cudaMalloc(&b->ptr, want);
+  if (e != cudaSuccess) {
+    b->ptr = nullptr;
+    return (int)e;
+  }
+  b->bytes = want;
+  return 0;
+}
+
+// Per-device state: CRC position tables, algo-2 tables, the soft buffer and
+// staging buffers of the single-code-block ABI, and per-stream scratch.
+struct DeviceState {
+  bool init = false;
+  uint32_t* crc_tab = nullptr;      // [4][kMaxB]
+  Buffer trained_dev[2];
+  uint64_t trained_gen[2] = {0, 0};
+  // single-code-block ABI
+  int16_t* harq = nullptr;          // [68*384] int16, process-wide soft buffer
+  Buffer one_llr, one_bits, one_stat;
+  cudaStream_t one_stream = nullptr;
+  // host-buffer batched API
+  struct HostStage {
+    Buffer llr, bits, stat, iters;
+  };
+  std::map<cudaStream_t, HostStage> host_stage;
+  std::map<cudaStream_t, Buffer> scratch;
+  int num_sms = 0;
+};
+
+std::map<int, DeviceState> g_dev;
+
+int device_state(DeviceState** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  DeviceState& st = g_dev[dev];
+  if (!st.init) {
+    e = cudaDeviceGetAttribute(&st.num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return (int)e;
+    std::vector<uint32_t> tab((size_t)4 * kMaxB);
+    for (int t = 0; t < 4; ++t) crc_position_table(t, tab.data() + (size_t)t * kMaxB);
+    e = cudaMalloc(&st.crc_tab, tab.size() * sizeof(uint32_t));
+    if (e != cudaSuccess) return (int)e;
+    e = cudaMemcpy(st.crc_tab, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return (int)e;
+    e = cudaMalloc(&st.harq, sizeof(int16_t) * kMaxCols * kMaxZc);
+    if (e != cudaSuccess) return (int)e;
+    e = cudaMemset(st.harq, 0, sizeof(int16_t) * kMaxCols * kMaxZc);
+    if (e != cudaSuccess) return (int)e;
+    e = cudaStreamCreateWithFlags(&st.one_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return (int)e;
+    st.init = true;
+  }
+  *out = &st;
+  return 0;
+}
+
+int trained_device_table(DeviceState* st, int bgn, const uint32_t** ptr, int* T) {
+  TrainedTable& t = trained(bgn);
+  const int k = bgn == 1 ? 0 : 1;
+  if (st->trained_gen[k] != t.generation) {
+    int e = ensure(&st->trained_dev[k], t.ab.size() * sizeof(uint32_t));
+    if (e) return e;
+    cudaError_t ce = cudaMemcpy(st->trained_dev[k].ptr, t.ab.data(), t.ab.size() * sizeof(uint32_t),
+                                cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return (int)ce;
+    st->trained_gen[k] = t.generation;
+  }
+  *ptr = static_cast<const uint32_t*>(st->trained_dev[k].ptr);
+  *T = t.T;
+  return 0;
+}
+
+struct Plan {
+  DecodeParams p;
+  int grid, block, smem;
+  bool degen;
+  int algo;
+  size_t scratch_bytes;
+};
+
+// Fill the launch parameters of one uniform batch.
+int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, DeviceState* st, Plan* plan) {
+  DecodeParams& p = plan->p;
+  memset(&p, 0, sizeof(p));
+  const BaseGraph& g = base_graph(cp.bgn);
+  p.Zc = cp.Zc;
+  p.R = g.rows;
+  p.lq_len = cp.lq_len;
+  p.B = cp.B;
+  p.K = cp.K;
+  p.F = cp.F;
+  p.N = cp.N;
+  p.Nv = cp.Nv;
+  p.E = cp.E;
+  p.Qm = cp.Qm;
+  p.symbols = cp.symbols;
+  p.c0 = cp.c0;
+  p.max_it = dc.max_iterations;
+  p.harq_on = cp.harq_on;
+  p.fill = dc.filling_bit_value;
+  p.max_llr = dc.max_llr;
+  p.min_llr = dc.min_llr;
+  p.crc_tab = st->crc_tab + (size_t)cp.crctype * kMaxB;
+  for (int e = 0; e < g.nnz; ++e) {
+    const uint32_t colbase = (uint32_t)g.col[e] * (uint32_t)cp.Zc;
+    const uint32_t sh = (uint32_t)(g.vij[cp.iLS][e] % cp.Zc);
+    p.edge[e] = colbase | (sh << 16);
+  }
+  for (int r = 0; r <= g.rows; ++r) p.row_off[r] = g.row_off[r];
+
+  const int algo = dc.algo;
+  plan->algo = algo;
+  const bool fixed = algo == 1 || algo == 2 || algo == 3;
+  p.G = std::max(1, kThreadsTarget / cp.Zc);
+  p.nact = p.G * cp.Zc;
+  plan->block = (p.nact + 31) & ~31;
+  plan->smem = p.G * cp.lq_len * 4;
+  p.num_cw = num_cw;
+  if (fixed) {
+    const int pairs = (num_cw + 1) / 2;
+    p.num_items = (pairs + p.G - 1) / p.G;
+  } else {
+    p.num_items = (num_cw + p.G - 1) / p.G;
+  }
+  // Alpha/beta source.
+  const int16_t alpha = (int16_t)dc.alpha;
+  const int16_t beta = (int16_t)dc.beta;
+  if (algo == 1) {
+    for (int r = 0; r < g.rows; ++r) p.w_inline[r] = pack_ab(alpha, beta);
+  } else if (algo == 3) {
+    for (int r = 0; r < g.rows; ++r) p.w_inline[r] = pack_ab(degree_alpha(g.degree[r]), beta);
+  } else if (algo == 2) {
+    int e = trained_device_table(st, cp.bgn, &p.weights, &p.weights_T);
+    if (e) return e;
+  }
+  p.f_alpha = (float)dc.alpha / 32768.0f;
+  p.f_beta = (float)dc.beta / 128.0f;
+  p.f_max = (float)dc.max_llr / 128.0f;
+  p.f_min = (float)dc.min_llr / 128.0f;
+  plan->degen = dc.min_llr > dc.max_llr;
+
+  // Scratch layout per CTA, layer by layer.
+  uint32_t off = 0;
+  for (int r = 0; r < g.rows; ++r) {
+    p.lr_off[r] = off;
+    const int deg = g.degree[r];
+    int planes;
+    if (algo == 0) {
+      planes = deg;
+    } else if (fixed) {
+      planes = deg > 16 ? 5 : 4;
+    } else {
+      planes = 4;
+    }
+    off += (uint32_t)planes * (uint32_t)p.nact;
+  }
+  p.lr_off[g.rows] = off;
+  p.scratch_words = off;
+
+  int occ;
+  if (fixed) {
+    occ = occupancy_fixed(plan->block, plan->smem, plan->degen);
+  } else if (algo == 4) {
+    occ = occupancy_float_minsum(plan->block, plan->smem);
+  } else {
+    occ = occupancy_float_bp(plan->block, plan->smem);
+  }
+  if (occ < 1) occ = 1;
+  plan->grid = std::min(p.num_items, occ * st->num_sms);
+  if (plan->grid < 1) plan->grid = 1;
+  plan->scratch_bytes = (size_t)plan->grid * (size_t)p.scratch_words * sizeof(uint32_t);
+  return 0;
+}
+
+int launch_plan(Plan* plan, void* stream) {
+  switch (plan->algo) {
+    case 1:
+    case 2:
+    case 3:
+      return launch_fixed(plan->p, plan->grid, plan->block, plan->smem, plan->degen, stream);
+    case 4:
+      return launch_float_minsum(plan->p, plan->grid, plan->block, plan->smem, stream);
+    default:
+      return launch_float_bp(plan->p, plan->grid, plan->block, plan->smem, stream);
+  }
+}
+
+int scratch_for(DeviceState* st, cudaStream_t s, size_t bytes, uint32_t** out) {
+  Buffer& b = st->scratch[s];
+  int e = ensure(&b, bytes);
+  if (e) return e;
+  *out = static_cast<uint32_t*>(b.ptr);
+  return 0;
+}
+
+// Shared body of the batched entry points.  `lock` must be held.
+int32_t decode_batch_locked(const int16_t* d_llr, int64_t llr_stride, int32_t num_cw,
+                            const ldpc_in_config_t* in, const ldpc_decoder_cfg_t* dc, uint8_t* d_bits,
+                            int64_t bits_stride, int32_t* d_status, int32_t* d_iters, void* d_app,
+                            int64_t app_stride, int16_t* d_harq, int64_t harq_stride, void* stream) {
+  if (!in || !dc || num_cw < 0) return NRLDPC_ERR_ARG;
+  CodeParams cp;
+  if (derive_params(*in, &cp, true) != 0) return NRLDPC_ERR_CONFIG;
+  if (dc->algo > 4) {
+    fprintf(stderr, "nrldpc: invalid decoding algorithm selection: %u\n", dc->algo);
+    return NRLDPC_ERR_ALGO;
+  }
+  if (num_cw == 0) return NRLDPC_OK;
+  if (!d_llr || llr_stride < cp.E) return NRLDPC_ERR_ARG;
+  if (d_bits && bits_stride < (cp.B + 7) / 8) return NRLDPC_ERR_ARG;
+  if (d_app && app_stride < cp.lq_len) return NRLDPC_ERR_ARG;
+  if (d_harq && harq_stride < cp.lq_len) return NRLDPC_ERR_ARG;
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
+  Plan plan;
+  if (make_plan(cp, *dc, num_cw, st, &plan) != 0) return NRLDPC_ERR_CUDA;
+  uint32_t* scratch = nullptr;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (scratch_for(st, s, plan.scratch_bytes, &scratch) != 0) return NRLDPC_ERR_CUDA;
+  DecodeParams& p = plan.p;
+  p.llr = d_llr;
+  p.llr_stride = llr_stride;
+  p.bits = d_bits;
+  p.bits_stride = bits_stride;
+  p.status = d_status;
+  p.iters = d_iters;
+  p.app = d_app;
+  p.app_stride = app_stride;
+  p.harq = d_harq;
+  p.harq_stride = harq_stride;
+  p.scratch = scratch;
+  if (launch_plan(&plan, stream) != 0) return NRLDPC_ERR_CUDA;
+  return NRLDPC_OK;
+}
+
+// One code block from host memory, through the process-wide soft buffer.
+int32_t decode_one(int16_t* LLr, uint8_t* hardbits, ldpc_in_config_t* inconfig, ldpc_decoder_cfg_t* dcfg) {
+  if (!inconfig || !dcfg) return NRLDPC_ERR_CONFIG;
+  CodeParams cp;
+  if (derive_params(*inconfig, &cp, true) != 0) return NRLDPC_ERR_CONFIG;
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
+  if (cp.E > 0 && !LLr) return NRLDPC_ERR_CUDA;
+  const int nbytes = (cp.B + 7) / 8;
+  if (ensure(&st->one_llr, sizeof(int16_t) * std::max(cp.E, 1)) || ensure(&st->one_bits, (size_t)nbytes) ||
+      ensure(&st->one_stat, 2 * sizeof(int32_t)))
+    return NRLDPC_ERR_CUDA;
+  cudaStream_t s = st->one_stream;
+  if (cp.E > 0 &&
+      cudaMemcpyAsync(st->one_llr.ptr, LLr, sizeof(int16_t) * cp.E, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  // The reference recovers into its soft buffer before it looks at algo
+  // (c_lib/c_ldpc_5g_decoder.c:44-78), so an invalid algo still updates the
+  // buffer: run the recovery alone (zero iterations) in that case.
+  ldpc_decoder_cfg_t run = *dcfg;
+  const bool bad_algo = dcfg->algo > 4;
+  if (bad_algo) {
+    run.algo = 1;
+    run.max_iterations = 0;
+  }
+  int32_t* d_stat = static_cast<int32_t*>(st->one_stat.ptr);
+  int32_t rc = decode_batch_locked(static_cast<int16_t*>(st->one_llr.ptr), std::max(cp.E, 1), 1, inconfig,
+                                   &run, static_cast<uint8_t*>(st->one_bits.ptr), nbytes, d_stat, nullptr,
+                                   nullptr, 0, st->harq, kMaxCols * kMaxZc, s);
+  if (rc != NRLDPC_OK) return rc;
+  int32_t status = 1;
+  if (cudaMemcpyAsync(&status, d_stat, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  // With zero iterations the reference leaves the caller's bits untouched.
+  if (run.max_iterations > 0 && hardbits &&
+      cudaMemcpyAsync(hardbits, st->one_bits.ptr, nbytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return NRLDPC_ERR_CUDA;
+  if (bad_algo) {
+    fprintf(stderr, "nrldpc: invalid decoding algorithm selection: %u\n", dcfg->algo);
+    return NRLDPC_ERR_ALGO;
+  }
+  return status;
+}
+
+}  // namespace
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+}  // namespace nrldpc
+
+using namespace nrldpc;
+
+extern "C" {
+
+int gen_ldpc_parameters(ldpc_config_t* params, ldpc_in_config_t* inconfig) {
+  if (!params || !inconfig) return -1;
+  params->bgn = inconfig->bgn;
+  params->A = inconfig->A;
+  params->crctype = inconfig->crctype;
+  params->E = inconfig->E;
+  params->rv = inconfig->rv;
+  params->Qm = inconfig->Qm;
+  params->HARQ_on = inconfig->HARQ_on;
+  CodeParams cp;
+  if (derive_params(*inconfig, &cp, true) != 0) return -1;
+  params->B = (uint16_t)cp.B;
+  params->Zc = (uint16_t)cp.Zc;
+  params->iLS = (uint16_t)cp.iLS;
+  params->K = (uint16_t)cp.K;
+  params->F = (uint16_t)cp.F;
+  params->N = (uint16_t)cp.N;
+  params->k0 = (uint16_t)cp.k0;
+  BaseGraph& g = const_cast<BaseGraph&>(base_graph(cp.bgn));
+  params->Vij_array = g.vij[cp.iLS];
+  params->HBG_array = g.col;
+  params->HBG_offset_array = g.row_off;
+  return 0;
+}
+
+uint32_t calculate_crc(const uint8_t* data, int len, int crctype) { return crc_remainder(data, len, crctype); }
+
+int32_t cuda_ldpc_5g_decode(int16_t* LLr, uint8_t* hardbits, ldpc_in_config_t* inconfig,
+                            ldpc_decoder_cfg_t* decoder_config) {
+  return decode_one(LLr, hardbits, inconfig, decoder_config);
+}
+
+int32_t c_ldpc_5g_decode(int16_t* LLr, uint8_t* hardbits, ldpc_in_config_t* inconfig,
+                         ldpc_decoder_cfg_t* decoder_config) {
+  return decode_one(LLr, hardbits, inconfig, decoder_config);
+}
+
+int32_t nrldpc_decode_batch(const int16_t* d_llr, int64_t llr_stride, int32_t num_cw,
+                            const ldpc_in_config_t* inconfig, const ldpc_decoder_cfg_t* decoder_cfg,
+                            uint8_t* d_hardbits, int64_t bits_stride, int32_t* d_status, int32_t* d_iterations,
+                            void* d_app, int64_t app_stride, int16_t* d_harq, int64_t harq_stride,
+                            void* stream) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  return decode_batch_locked(d_llr, llr_stride, num_cw, inconfig, decoder_cfg, d_hardbits, bits_stride, d_status,
+                             d_iterations, d_app, app_stride, d_harq, harq_stride, stream);
+}
+
+int32_t nrldpc_decode_batch_host(const int16_t* h_llr, int64_t llr_stride, int32_t num_cw,
+                                 const ldpc_in_config_t* inconfig, const ldpc_decoder_cfg_t* decoder_cfg,
+                                 uint8_t* h_hardbits, int64_t bits_stride, int32_t* h_status,
+                                 int32_t* h_iterations, void* stream) {
+  if (!inconfig || !decoder_cfg || num_cw < 0) return NRLDPC_ERR_ARG;
+  CodeParams cp;
+  if (derive_params(*inconfig, &cp, true) != 0) return NRLDPC_ERR_CONFIG;
+  if (decoder_cfg->algo > 4) return NRLDPC_ERR_ALGO;
+  if (num_cw == 0) return NRLDPC_OK;
+  if (!h_llr || llr_stride < cp.E || !h_hardbits) return NRLDPC_ERR_ARG;
+  const int nbytes = (cp.B + 7) / 8;
+  if (bits_stride < nbytes) return NRLDPC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  DeviceState::HostStage& hs = st->host_stage[s];
+  const size_t llr_bytes = sizeof(int16_t) * (size_t)num_cw * (size_t)llr_stride;
+  const size_t bit_bytes = (size_t)num_cw * (size_t)bits_stride;
+  if (ensure(&hs.llr, llr_bytes) || ensure(&hs.bits, bit_bytes) || ensure(&hs.stat, sizeof(int32_t) * num_cw) ||
+      ensure(&hs.iters, sizeof(int32_t) * num_cw))
+    return NRLDPC_ERR_CUDA;
+  if (cudaMemcpyAsync(hs.llr.ptr, h_llr, llr_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  int32_t rc = decode_batch_locked(static_cast<int16_t*>(hs.llr.ptr), llr_stride, num_cw, inconfig, decoder_cfg,
+                                   static_cast<uint8_t*>(hs.bits.ptr), bits_stride,
+                                   static_cast<int32_t*>(hs.stat.ptr), static_cast<int32_t*>(hs.iters.ptr), nullptr,
+                                   0, nullptr, 0, stream);
+  if (rc != NRLDPC_OK) return rc;
+  if (decoder_cfg->max_iterations > 0 &&
+      cudaMemcpyAsync(h_hardbits, hs.bits.ptr, bit_bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  if (h_status &&
+      cudaMemcpyAsync(h_status, hs.stat.ptr, sizeof(int32_t) * num_cw, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  if (h_iterations &&
+      cudaMemcpyAsync(h_iterations, hs.iters.ptr, sizeof(int32_t) * num_cw, cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return NRLDPC_ERR_CUDA;
+  return NRLDPC_OK;
+}
+
+int32_t nrldpc_set_trained_weights(uint16_t bgn, const int16_t* alpha, const int16_t* beta,
+                                   int32_t num_iterations) {
+  if (bgn != 1 && bgn != 2) return NRLDPC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_mu);
+  TrainedTable& t = g_trained[bgn == 1 ? 0 : 1];
+  if (!alpha) {
+    default_trained(bgn, &t);
+    return NRLDPC_OK;
+  }
+  if (num_iterations < 1 || num_iterations > 65535) return NRLDPC_ERR_ARG;
+  const BaseGraph& g = base_graph(bgn);
+  t.T = num_iterations;
+  t.ab.assign((size_t)num_iterations * g.rows, 0u);
+  for (size_t i = 0; i < t.ab.size(); ++i) t.ab[i] = pack_ab(alpha[i], beta ? beta[i] : (int16_t)0);
+  t.generation = g_trained_gen++;
+  return NRLDPC_OK;
+}
+
+int32_t nrldpc_set_degree_alpha(const int16_t* degree_alpha_values) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  memcpy(g_degree_alpha, degree_alpha_values ? degree_alpha_values : kDefaultDegreeAlpha, sizeof(g_degree_alpha));
+  g_degree_alpha_init = true;
+  return NRLDPC_OK;
+}
+
+int64_t nrldpc_kernel_launch_count(void) { return g_launches.load(); }
+
+const char* nrldpc_version(void) { return "nrldpc-b200 0.1.0 (sm_100a)"; }
+
+}  // extern "C"

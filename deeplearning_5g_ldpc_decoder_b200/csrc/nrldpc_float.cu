@@ -1,0 +1,315 @@
+// nrldpc_float.cu — FP32 layered decoders for sm_100a: float min-sum (algo 4)
+// and belief propagation (algo 0).
+//
+// Semantics follow c_lib/floatpoint_ldpc_decoder.c.  Float min-sum
+// (:163-220, :307-366) is reproduced operation for operation with
+// round-to-nearest intrinsics (no FMA contraction), so it is bit-exact.  BP
+// (:53-151, :237-298) uses tanh/atanh; those are evaluated in double precision
+// and rounded to float, which differs from the host libm's tanhf/atanhf by at
+// most an ulp now and then, so BP matches the reference to a tolerance.
+//
+// Mapping: one code block per group of Zc threads, G = floor(384 / Zc) groups
+// per CTA, FP32 beliefs in shared memory, persistent grid.  Min-sum messages
+// are stored compressed per lifted check row (two minima, flip bits, the
+// minimum's position: 16 bytes); BP messages are stored per edge.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "nrldpc_decode_common.cuh"
+#include "nrldpc_internal.h"
+
+namespace nrldpc {
+namespace {
+
+constexpr float kBpAtanhClip = 19.07f;   // c_lib/floatpoint_ldpc_decoder.c:31
+
+__device__ __forceinline__ float clipf(float v, float mx, float mn) {
+  // clip_float_llr (c_lib/floatpoint_ldpc_decoder.c:153-161)
+  return v > mx ? mx : (v < mn ? mn : v);
+}
+
+__device__ __forceinline__ uint32_t edge_addr(const DecodeParams& p, int e, uint32_t zx) {
+  const uint32_t ed = p.edge[e];
+  uint32_t t = zx + (ed >> 16);
+  t = min(t, t - (uint32_t)p.Zc);
+  return (ed & 0xFFFFu) + t;
+}
+
+// ---------------------------------------------------------------- float min-sum
+// Stored message of a lifted check row (4 planes): new_min1, new_min2 (float
+// bits), bit j = message of edge j negated, bit j = edge j carries new_min2.
+template <int D>
+__device__ __forceinline__ void fms_row(const DecodeParams& p, float* __restrict__ lq, uint32_t zx, int e0,
+                                        bool first, uint32_t* __restrict__ lrp, int NT) {
+  float n1 = 0.f, n2 = 0.f;
+  uint32_t xf = 0u, xi = 0u;
+  if (!first) {
+    n1 = __uint_as_float(lrp[0]);
+    n2 = __uint_as_float(lrp[NT]);
+    xf = lrp[2 * NT];
+    xi = lrp[3 * NT];
+  }
+  float rel[D];
+  uint32_t addr[D];
+  float m1 = FLT_MAX, m2 = FLT_MAX;
+  int idx = 0;
+  bool neg = false;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    addr[j] = edge_addr(p, e0 + j, zx);
+    float r = ((xi >> j) & 1u) ? n2 : n1;
+    r = ((xf >> j) & 1u) ? -r : r;
+    const float v = __fsub_rn(lq[addr[j]], r);
+    rel[j] = v;
+    neg ^= (v < 0.0f);
+    const float a = fabsf(v);
+    // float_update_two_minima (:171-180): strict <, first index wins.
+    if (a < m1) {
+      m2 = m1;
+      m1 = a;
+      idx = j;
+    } else if (a < m2) {
+      m2 = a;
+    }
+  }
+  const float c1 = clipf(m1, p.f_max, 0.0f);
+  const float c2 = clipf(m2, p.f_max, 0.0f);
+  float o1 = __fsub_rn(c1, p.f_beta);
+  float o2 = __fsub_rn(c2, p.f_beta);
+  o1 = o1 < 0.0f ? 0.0f : o1;
+  o2 = o2 < 0.0f ? 0.0f : o2;
+  const float s1 = __fmul_rn(p.f_alpha, o1);
+  const float s2 = __fmul_rn(p.f_alpha, o2);
+  uint32_t XF = 0u;
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    const float nv = (j == idx) ? s2 : s1;
+    const bool flip = (rel[j] < 0.0f) != neg;
+    const float msg = flip ? -nv : nv;      // edge_sign * new_val, edge_sign = +-1
+    XF |= (flip ? 1u : 0u) << j;
+    lq[addr[j]] = clipf(__fadd_rn(rel[j], msg), p.f_max, p.f_min);
+  }
+  lrp[0] = __float_as_uint(s1);
+  lrp[NT] = __float_as_uint(s2);
+  lrp[2 * NT] = XF;
+  lrp[3 * NT] = 1u << idx;
+}
+
+__device__ __forceinline__ void fms_dispatch(int deg, const DecodeParams& p, float* lq, uint32_t zx, int e0,
+                                             bool first, uint32_t* lrp, int NT) {
+  switch (deg) {
+    case 3: fms_row<3>(p, lq, zx, e0, first, lrp, NT); break;
+    case 4: fms_row<4>(p, lq, zx, e0, first, lrp, NT); break;
+    case 5: fms_row<5>(p, lq, zx, e0, first, lrp, NT); break;
+    case 6: fms_row<6>(p, lq, zx, e0, first, lrp, NT); break;
+    case 7: fms_row<7>(p, lq, zx, e0, first, lrp, NT); break;
+    case 8: fms_row<8>(p, lq, zx, e0, first, lrp, NT); break;
+    case 9: fms_row<9>(p, lq, zx, e0, first, lrp, NT); break;
+    case 10: fms_row<10>(p, lq, zx, e0, first, lrp, NT); break;
+    default: fms_row<19>(p, lq, zx, e0, first, lrp, NT); break;
+  }
+}
+
+// --------------------------------------------------------------------- BP
+__device__ __forceinline__ float bp_message(float prod) {
+  // bp_message_from_product (:54-62)
+  if (prod >= 1.0f) return 2.0f * kBpAtanhClip;
+  if (prod <= -1.0f) return -2.0f * kBpAtanhClip;
+  return __fmul_rn(2.0f, (float)atanh((double)prod));
+}
+
+template <int D>
+__device__ __forceinline__ void bp_row(const DecodeParams& p, float* __restrict__ lq, uint32_t zx, int e0,
+                                       bool first, uint32_t* __restrict__ lrp, int NT) {
+  float rel[D], th[D];
+  uint32_t addr[D];
+  int nz = 0, zidx = -1;
+  float nzprod = 1.0f;
+  // compute_tanh_values (:65-82): tanh(rel/2), zero count, product of non-zeros.
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    addr[j] = edge_addr(p, e0 + j, zx);
+    const float old = first ? 0.0f : __uint_as_float(lrp[j * NT]);
+    const float v = __fsub_rn(lq[addr[j]], old);
+    rel[j] = v;
+    if (v == 0.0f) {
+      ++nz;
+      zidx = j;
+      th[j] = 0.0f;
+    } else {
+      th[j] = (float)tanh((double)__fmul_rn(v, 0.5f));
+      nzprod = __fmul_rn(nzprod, th[j]);
+    }
+  }
+  float msg[D];
+  if (nz == 1) {
+#pragma unroll
+    for (int j = 0; j < D; ++j) msg[j] = 0.0f;
+    const float m = bp_message(nzprod);
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+      if (j == zidx) msg[j] = m;
+  } else if (nz >= 2) {
+#pragma unroll
+    for (int j = 0; j < D; ++j) msg[j] = 0.0f;
+  } else {
+    // prefix/suffix products (:85-96, :135-145), same multiplication order.
+    float pre[D + 1], suf[D + 1];
+    pre[0] = 1.0f;
+#pragma unroll
+    for (int j = 0; j < D; ++j) pre[j + 1] = __fmul_rn(pre[j], th[j]);
+    suf[D] = 1.0f;
+#pragma unroll
+    for (int j = D - 1; j >= 0; --j) suf[j] = __fmul_rn(suf[j + 1], th[j]);
+#pragma unroll
+    for (int j = 0; j < D; ++j) msg[j] = bp_message(__fmul_rn(pre[j], suf[j + 1]));
+  }
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    lrp[j * NT] = __float_as_uint(msg[j]);
+    lq[addr[j]] = __fadd_rn(rel[j], msg[j]);   // no clipping in BP (:148-150)
+  }
+}
+
+__device__ __forceinline__ void bp_dispatch(int deg, const DecodeParams& p, float* lq, uint32_t zx, int e0,
+                                            bool first, uint32_t* lrp, int NT) {
+  switch (deg) {
+    case 3: bp_row<3>(p, lq, zx, e0, first, lrp, NT); break;
+    case 4: bp_row<4>(p, lq, zx, e0, first, lrp, NT); break;
+    case 5: bp_row<5>(p, lq, zx, e0, first, lrp, NT); break;
+    case 6: bp_row<6>(p, lq, zx, e0, first, lrp, NT); break;
+    case 7: bp_row<7>(p, lq, zx, e0, first, lrp, NT); break;
+    case 8: bp_row<8>(p, lq, zx, e0, first, lrp, NT); break;
+    case 9: bp_row<9>(p, lq, zx, e0, first, lrp, NT); break;
+    case 10: bp_row<10>(p, lq, zx, e0, first, lrp, NT); break;
+    default: bp_row<19>(p, lq, zx, e0, first, lrp, NT); break;
+  }
+}
+
+__device__ void emit_float_block(const DecodeParams& p, const float* lq, int zx, int cw, int status, int iters) {
+  if (iters > 0 && p.bits) {
+    const int nbytes = (p.B + 7) >> 3;
+    uint8_t* out = p.bits + (int64_t)cw * p.bits_stride;
+    for (int byte = zx; byte < nbytes; byte += p.Zc) {
+      uint32_t v = 0u;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const int i = byte * 8 + b;
+        v = (v << 1) | ((i < p.B && lq[i] < 0.0f) ? 1u : 0u);
+      }
+      out[byte] = (uint8_t)v;
+    }
+  }
+  if (p.app) {
+    float* out = reinterpret_cast<float*>(p.app) + (int64_t)cw * p.app_stride;
+    for (int i = zx; i < p.lq_len; i += p.Zc) out[i] = lq[i];
+  }
+  if (zx == 0) {
+    if (p.status) p.status[cw] = status;
+    if (p.iters) p.iters[cw] = iters;
+  }
+}
+
+template <bool kBP>
+__global__ void __launch_bounds__(kThreadsTarget) float_kernel(const __grid_constant__ DecodeParams p) {
+  extern __shared__ __align__(16) float s_lqf[];     // [G][lq_len]
+  __shared__ uint32_t s_crc[kMaxGroups];
+
+  const int tid = threadIdx.x;
+  const int g = tid / p.Zc;
+  const int zx = tid - g * p.Zc;
+  const bool active = g < p.G;
+  float* lq = s_lqf + (active ? g : 0) * p.lq_len;
+  uint32_t* scratch = p.scratch + (int64_t)blockIdx.x * p.scratch_words;
+  const int NT = p.nact;
+  const int Bp = (p.B + 31) & ~31;
+
+  for (int item = blockIdx.x; item < p.num_items; item += gridDim.x) {
+    const int cw = item * p.G + g;
+    const bool valid = active && cw < p.num_cw;
+    if (active) {
+      const int16_t* in = p.llr + (int64_t)(valid ? cw : 0) * p.llr_stride;
+      int16_t* hq = (p.harq && valid) ? p.harq + (int64_t)cw * p.harq_stride : nullptr;
+      for (int i = zx; i < p.lq_len; i += p.Zc) {
+        int32_t a = (p.harq_on && hq) ? hq[i] : 0;
+        a = valid ? recover_position(p, in, i, a) : 0;
+        if (hq) hq[i] = (int16_t)a;
+        // dequantize_int16_to_llr (c_lib/tx_rx_process.c:42-44): exact.
+        lq[i] = __fdiv_rn((float)(int16_t)a, 128.0f);
+      }
+    }
+    if (tid < kMaxGroups) s_crc[tid] = 0u;
+    bool done = !valid;
+    __syncthreads();
+
+    int it = 0;
+    for (; it < p.max_it; ++it) {
+      for (int row = 0; row < p.R; ++row) {
+        if (active) {
+          const int e0 = p.row_off[row];
+          const int deg = p.row_off[row + 1] - e0;
+          uint32_t* lrp = scratch + p.lr_off[row] + tid;
+          if (kBP) {
+            bp_dispatch(deg, p, lq, (uint32_t)zx, e0, it == 0, lrp, NT);
+          } else {
+            fms_dispatch(deg, p, lq, (uint32_t)zx, e0, it == 0, lrp, NT);
+          }
+        }
+        __syncthreads();
+      }
+      for (int k = tid; k < p.G * Bp; k += blockDim.x) {
+        const int gg = k / Bp;
+        const int i = k - gg * Bp;
+        uint32_t r = 0u;
+        if (i < p.B && s_lqf[gg * p.lq_len + i] < 0.0f) r = crc_term(p, i);
+        r = __reduce_xor_sync(0xFFFFFFFFu, r);
+        if ((tid & 31) == 0 && r) atomicXor(&s_crc[gg], r);
+      }
+      __syncthreads();
+      if (active && !done && s_crc[g] == 0u) {
+        emit_float_block(p, lq, zx, cw, 0, it + 1);
+        done = true;
+      }
+      const bool all_done = __syncthreads_and(done);
+      if (tid < kMaxGroups) s_crc[tid] = 0u;
+      if (all_done) {
+        ++it;
+        break;
+      }
+    }
+    if (active && !done) emit_float_block(p, lq, zx, cw, 1, it);
+    __syncthreads();
+  }
+}
+
+template <typename K>
+int launch_impl(K kernel, const DecodeParams& p, int grid, int block, int smem, void* stream) {
+  cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (err != cudaSuccess) return (int)err;
+  kernel<<<grid, block, smem, reinterpret_cast<cudaStream_t>(stream)>>>(p);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+template <typename K>
+int occupancy_impl(K kernel, int block, int smem) {
+  int n = 0;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, smem);
+  return n;
+}
+
+}  // namespace
+
+int launch_float_minsum(const DecodeParams& p, int grid, int block, int smem, void* stream) {
+  return launch_impl(float_kernel<false>, p, grid, block, smem, stream);
+}
+int launch_float_bp(const DecodeParams& p, int grid, int block, int smem, void* stream) {
+  return launch_impl(float_kernel<true>, p, grid, block, smem, stream);
+}
+int occupancy_float_minsum(int block, int smem) { return occupancy_impl(float_kernel<false>, block, smem); }
+int occupancy_float_bp(int block, int smem) { return occupancy_impl(float_kernel<true>, block, smem); }
+
+}  // namespace nrldpc

@@ -1,0 +1,105 @@
+// nrldpc_internal.h — definitions shared by the host glue and the CUDA kernels.
+#pragma once
+
+#include <stdint.h>
+
+#include "nrldpc_b200.h"
+
+namespace nrldpc {
+
+constexpr int kMaxRows = NRLDPC_BG1_ROWS;   // 46
+constexpr int kMaxCols = NRLDPC_BG1_COLS;   // 68
+constexpr int kMaxNnz = NRLDPC_BG1_NNZ;     // 316
+constexpr int kMaxDegree = NRLDPC_MAX_DEGREE;
+constexpr int kMaxZc = NRLDPC_MAX_ZC;
+constexpr int kMaxB = 8448;                  // BG1 K at Zc=384
+constexpr int kThreadsTarget = 384;          // lifted rows handled by one CTA
+constexpr int kMaxGroups = kThreadsTarget / 2;  // Zc=2 packs 192 groups
+
+// One base graph with its CSR view (reference layout, for gen_ldpc_parameters)
+// and per-row degrees.
+struct BaseGraph {
+  int bgn, rows, cols, nnz;
+  uint16_t row_off[kMaxRows + 1];
+  uint16_t col[kMaxNnz];
+  uint16_t vij[8][kMaxNnz];
+  uint8_t degree[kMaxRows];
+};
+
+const BaseGraph& base_graph(int bgn);
+
+// Everything derived from ldpc_in_config_t that the kernels need.
+struct CodeParams {
+  int bgn, A, crctype, E, rv, Qm, harq_on;
+  int B, Zc, iLS, K, F, N, k0;
+  int rows, cols, nnz;
+  int lq_len;     // N + 2*Zc = cols*Zc
+  int Nv;         // N - F, non-filler positions of the circular buffer
+  int c0;         // start position k0 mapped into the compacted buffer
+  int symbols;    // E / Qm
+  int crc_w;      // 16 or 24
+};
+
+// Restatement of gen_ldpc_parameters' validation and derivation
+// (c_lib/ldpc_internal.c:66-170).  Returns 0 on success, -1 on a bad config.
+int derive_params(const ldpc_in_config_t& in, CodeParams* out, bool verbose);
+
+// Host CRC remainder (c_lib/nr_crc.c:129-179 semantics).
+uint32_t crc_remainder(const uint8_t* data, int len, int crctype);
+
+// T[d] = x^(d + W) mod g(x) for d in [0, kMaxB): the CRC remainder of a
+// message whose only set bit sits d positions before its end.
+void crc_position_table(int crctype, uint32_t* out /* kMaxB */);
+
+// Alpha/beta per (iteration, row): alpha in the low 16 bits, beta in the high.
+inline uint32_t pack_ab(int16_t alpha, int16_t beta) {
+  return (uint32_t)(uint16_t)alpha | ((uint32_t)(uint16_t)beta << 16);
+}
+
+// Launch parameters of every decode kernel.  Passed by value as a
+// __grid_constant__ kernel parameter so that the per-edge tables are read
+// through the constant cache with warp-uniform indices.
+struct DecodeParams {
+  int32_t Zc, R, lq_len, B, K, F, N, Nv, E, Qm, symbols, c0, max_it;
+  int32_t G;      // codeword slots per CTA: pairs (fixed point) or codewords (float)
+  int32_t nact;   // active threads per CTA = G * Zc
+  int32_t num_cw, num_items;
+  int32_t harq_on;
+  int32_t fill, max_llr, min_llr;
+  int32_t weights_T;   // 0: use w_inline[row]; >0: weights[min(it,T-1)*R + row]
+  float f_alpha, f_beta, f_max, f_min;
+  const uint32_t* weights;
+  const uint32_t* crc_tab;
+  const int16_t* llr;
+  int64_t llr_stride;
+  uint8_t* bits;
+  int64_t bits_stride;
+  int32_t* status;
+  int32_t* iters;
+  void* app;
+  int64_t app_stride;
+  int16_t* harq;
+  int64_t harq_stride;
+  uint32_t* scratch;
+  int64_t scratch_words;   // per CTA
+  // Per edge: (base column * Zc) in the low 16 bits, (V_ij mod Zc) in the high.
+  uint32_t edge[kMaxNnz];
+  uint32_t lr_off[kMaxRows + 1];   // per-layer word offset inside a CTA's scratch
+  uint32_t w_inline[kMaxRows];
+  uint16_t row_off[kMaxRows + 1];
+};
+
+// Kernel launchers (defined in the .cu files).  Return a cudaError_t value.
+int launch_fixed(const DecodeParams& p, int grid, int block, int smem, bool degen_clip,
+                 void* stream);
+int launch_float_minsum(const DecodeParams& p, int grid, int block, int smem, void* stream);
+int launch_float_bp(const DecodeParams& p, int grid, int block, int smem, void* stream);
+
+// Occupancy helpers (per kernel variant).
+int occupancy_fixed(int block, int smem, bool degen_clip);
+int occupancy_float_minsum(int block, int smem);
+int occupancy_float_bp(int block, int smem);
+
+void count_launch();
+
+}  // namespace nrldpc

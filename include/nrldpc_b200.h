@@ -1,0 +1,192 @@
+/*
+ * nrldpc_b200.h — C ABI of the B200 5G NR LDPC receive path.
+ *
+ * One shared library (deeplearning_5g_ldpc_decoder_b200/libnrldpc_b200.so)
+ * exports two groups of entry points:
+ *
+ *  1. Drop-in replacements for the reference library's C ABI.  Their
+ *     signatures, record layouts, argument meaning and return codes are those
+ *     of the reference's c_lib/nr_ldpc.h, so the reference's ctypes harness
+ *     (scripts/ldpc_c_sim_common.py:60-109) and table loader
+ *     (deep_learning/ldpc_table_config.py:93-154) bind them unchanged.
+ *
+ *  2. Batched, stream-ordered device entry points (nrldpc_*), which take
+ *     device pointers and a cudaStream_t and decode many codewords per call.
+ *
+ * Every decoder entry point runs on the GPU.  There is no CPU fallback: if no
+ * CUDA device is usable the calls return NRLDPC_ERR_CUDA (-1).
+ *
+ * Return codes (mirroring c_lib/c_ldpc_5g_decoder.c:16-32):
+ *    0  CRC passed within max_iterations
+ *    1  not converged (CRC still failing after max_iterations)
+ *   -1  CUDA / runtime error
+ *   -2  invalid LDPC configuration
+ *   -3  invalid decoder algorithm
+ *   -4  invalid argument to a batched entry point (bad pointer / size)
+ */
+#ifndef NRLDPC_B200_H
+#define NRLDPC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NRLDPC_OK 0
+#define NRLDPC_NOT_CONVERGED 1
+#define NRLDPC_ERR_CUDA (-1)
+#define NRLDPC_ERR_CONFIG (-2)
+#define NRLDPC_ERR_ALGO (-3)
+#define NRLDPC_ERR_ARG (-4)
+
+#define NRLDPC_BG1_ROWS 46
+#define NRLDPC_BG1_COLS 68
+#define NRLDPC_BG1_NNZ 316
+#define NRLDPC_BG2_ROWS 42
+#define NRLDPC_BG2_COLS 52
+#define NRLDPC_BG2_NNZ 197
+#define NRLDPC_MAX_DEGREE 19
+#define NRLDPC_MAX_ZC 384
+
+/* Caller-supplied code-block configuration.  Same layout as the reference's
+ * ldpc_in_config_t (c_lib/nr_ldpc.h:42-50): seven uint16_t, 14 bytes. */
+typedef struct {
+    uint16_t bgn;     /* base graph: 1 or 2 */
+    uint16_t A;       /* payload bits before CRC (multiple of 8) */
+    uint16_t crctype; /* 0 CRC16, 1 CRC24A, 2 CRC24B, 3 CRC24C */
+    uint16_t E;       /* rate-matched bits (multiple of Qm) */
+    uint16_t rv;      /* redundancy version 0..3 */
+    uint16_t Qm;      /* modulation order 1, 2, 4, 6 or 8 */
+    uint16_t HARQ_on; /* 1: add to the soft buffer, 0: start a fresh buffer */
+} ldpc_in_config_t;
+
+/* Derived parameters.  Same layout as the reference's ldpc_config_t
+ * (c_lib/nr_ldpc.h:54-79); the three table pointers point at this library's
+ * own copies of the base graph in the reference's CSR form (row offsets,
+ * column ids, raw shifts of the selected lifting set). */
+typedef struct {
+    uint16_t bgn, A, crctype, E, rv, Qm, HARQ_on;
+    uint16_t B, Zc, iLS, K, F, N, k0;
+    uint16_t *Vij_array;
+    uint16_t *HBG_array;
+    uint16_t *HBG_offset_array;
+} ldpc_config_t;
+
+/* Decoder settings, the row [algo, max_iterations, alpha, beta,
+ * filling_bit_value, max_llr, min_llr].  Same layout as the reference's
+ * ldpc_decoder_cfg_t (c_lib/nr_ldpc.h:82-90).  alpha and beta are unsigned at
+ * the ABI and reinterpreted as int16_t by the fixed-point decoders, exactly
+ * as the reference does (c_lib/fixedpoint_ldpc_decoder.c:207-209). */
+typedef struct {
+    uint16_t algo;           /* 0 BP, 1 min-sum, 2 trained min-sum, 3 degree min-sum, 4 float min-sum */
+    uint16_t max_iterations;
+    uint16_t alpha;          /* Q15 normalisation */
+    uint16_t beta;           /* offset, LLR units (x128 scale) */
+    int16_t filling_bit_value;
+    int16_t max_llr;
+    int16_t min_llr;
+} ldpc_decoder_cfg_t;
+
+/* ------------------------------------------------------------------------ */
+/* 1. Reference ABI                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* Validate a configuration and derive B, Zc, iLS, K, F, N, k0 and the table
+ * pointers.  Returns 0 or -1.  Replaces gen_ldpc_parameters
+ * (c_lib/nr_ldpc.h:108, c_lib/ldpc_internal.c:66-170). */
+int gen_ldpc_parameters(ldpc_config_t *params, ldpc_in_config_t *inconfig);
+
+/* Decode one code block from host memory: rate recovery (with HARQ combining
+ * into this library's process-wide soft buffer when HARQ_on=1), layered
+ * decoding with the selected algorithm, CRC early termination.  Writes
+ * ceil(B/8) bytes of hard decisions, MSB first.  Supports algo 0..4.
+ * Replaces cuda_ldpc_5g_decode (CUDA/cuda_ldpc_5g_decoder.cu:31-58), which
+ * supports only algo 1 and 4. */
+int32_t cuda_ldpc_5g_decode(int16_t *LLr, uint8_t *hardbits,
+                            ldpc_in_config_t *inconfig,
+                            ldpc_decoder_cfg_t *decoder_config);
+
+/* Same call under the C library's symbol name (c_lib/nr_ldpc.h:127,
+ * c_lib/c_ldpc_5g_decoder.c:34-79); it runs on the GPU as well. */
+int32_t c_ldpc_5g_decode(int16_t *LLr, uint8_t *hardbits,
+                         ldpc_in_config_t *inconfig,
+                         ldpc_decoder_cfg_t *decoder_config);
+
+/* Table-driven NR CRC remainder over len bytes, MSB first; 0 for an
+ * unknown crctype.  Host function.  Replaces calculate_crc
+ * (c_lib/nr_ldpc.h:102, c_lib/nr_crc.c:170-179). */
+uint32_t calculate_crc(const uint8_t *data, int len, int crctype);
+
+/* ------------------------------------------------------------------------ */
+/* 2. Batched device API (no counterpart in the reference, which decodes one */
+/*    code block per call)                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Decode num_cw code blocks that share one configuration.
+ *
+ *   d_llr        device int16 [num_cw][llr_stride], rate-matched order, E used
+ *   d_hardbits   device uint8 [num_cw][bits_stride], ceil(B/8) bytes written
+ *                (left untouched when max_iterations == 0, as the reference)
+ *   d_status     device int32 [num_cw]: 0 CRC pass, 1 not converged (nullable)
+ *   d_iterations device int32 [num_cw]: iterations executed (nullable)
+ *   d_app        device [num_cw][app_stride] final beliefs LQ, N+2*Zc values:
+ *                int16 for algos 1-3, float32 for algos 0 and 4 (nullable)
+ *   d_harq       device int16 [num_cw][harq_stride] per-codeword soft buffers
+ *                of N+2*Zc values (nullable).  When given, rate recovery starts
+ *                from it if inconfig->HARQ_on == 1, and the recovered buffer
+ *                is written back to it.
+ *   stream       cudaStream_t (NULL = legacy default stream)
+ *
+ * Stream-ordered: returns after enqueueing.  Scratch memory is owned by the
+ * library, one buffer per (device, stream).  Returns 0, -1, -2, -3 or -4. */
+int32_t nrldpc_decode_batch(const int16_t *d_llr, int64_t llr_stride,
+                            int32_t num_cw,
+                            const ldpc_in_config_t *inconfig,
+                            const ldpc_decoder_cfg_t *decoder_cfg,
+                            uint8_t *d_hardbits, int64_t bits_stride,
+                            int32_t *d_status, int32_t *d_iterations,
+                            void *d_app, int64_t app_stride,
+                            int16_t *d_harq, int64_t harq_stride,
+                            void *stream);
+
+/* Same as nrldpc_decode_batch, from and to HOST memory: copies the LLRs in,
+ * decodes, copies hard bits / status / iterations back and synchronises the
+ * stream.  Pinned host buffers give full copy bandwidth.  h_status and
+ * h_iterations are nullable. */
+int32_t nrldpc_decode_batch_host(const int16_t *h_llr, int64_t llr_stride,
+                                 int32_t num_cw,
+                                 const ldpc_in_config_t *inconfig,
+                                 const ldpc_decoder_cfg_t *decoder_cfg,
+                                 uint8_t *h_hardbits, int64_t bits_stride,
+                                 int32_t *h_status, int32_t *h_iterations,
+                                 void *stream);
+
+/* Replace the per-(iteration, row) alpha/beta tables used by algo 2 for one
+ * base graph (the reference compiles these in:
+ * c_lib/BG1_trained_ldpc_weights.c:34,171, c_lib/BG2_trained_ldpc_weights.c).
+ * alpha/beta are [num_iterations][rows] int16 Q15 / LLR units.  Iterations at
+ * or beyond num_iterations reuse the last table row.  Passing NULL alpha
+ * restores the built-in table.  Not safe to call while a decode is running. */
+int32_t nrldpc_set_trained_weights(uint16_t bgn, const int16_t *alpha,
+                                   const int16_t *beta, int32_t num_iterations);
+
+/* Replace the 19-entry degree->alpha table used by algo 3 (entry d-1 is the
+ * alpha of a degree-d row), as the reference's
+ * layered_degree_minsum_ldpc_decode_with_alpha
+ * (c_lib/degree_fixedpoint_ldpc_decoder.c:200-268) takes it per call.
+ * NULL restores the default table. */
+int32_t nrldpc_set_degree_alpha(const int16_t *degree_alpha);
+
+/* Number of CUDA kernels this library has launched in this process. */
+int64_t nrldpc_kernel_launch_count(void);
+
+/* Library version string. */
+const char *nrldpc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NRLDPC_B200_H */
