@@ -45,6 +45,11 @@ def code_params(inconfig) -> capi.LdpcConfig:
     return capi.gen_ldpc_parameters(_as_in_config(inconfig))
 
 
+def _row_stride(t: torch.Tensor) -> int:
+    """Elements between rows; torch leaves the stride of a size-1 dim arbitrary."""
+    return t.stride(0) if t.shape[0] > 1 else t.shape[1]
+
+
 def _check(rc: int, what: str) -> None:
     if rc == capi.NRLDPC_OK:
         return
@@ -66,8 +71,12 @@ def ldpc_decode(llr: torch.Tensor, inconfig, decoder_config, *, return_app: bool
     """
     cfg = _as_in_config(inconfig)
     dcfg = _as_decoder_config(decoder_config)
-    if not llr.is_cuda or llr.dtype != torch.int16 or llr.dim() != 2 or llr.stride(1) != 1:
-        raise ValueError("llr must be a row-contiguous int16 CUDA tensor of shape [n, L]")
+    if not llr.is_cuda or llr.dtype != torch.int16 or llr.dim() != 2:
+        raise ValueError("llr must be an int16 CUDA tensor of shape [n, L]")
+    if llr.shape[0] > 1 and (llr.stride(1) != 1 or llr.stride(0) < llr.shape[1]):
+        llr = llr.contiguous()
+    elif llr.shape[0] <= 1 and llr.stride(1) != 1:
+        llr = llr.contiguous()
     p = code_params(cfg)
     n = llr.shape[0]
     nb = (p.B + 7) // 8
@@ -88,13 +97,13 @@ def ldpc_decode(llr: torch.Tensor, inconfig, decoder_config, *, return_app: bool
     stream = torch.cuda.current_stream(dev).cuda_stream
     with torch.cuda.device(dev):
         rc = lib.nrldpc_decode_batch(
-            ctypes.c_void_p(llr.data_ptr()), llr.stride(0), n, ctypes.byref(cfg), ctypes.byref(dcfg),
-            ctypes.c_void_p(out.hardbits.data_ptr()), out.hardbits.stride(0),
+            ctypes.c_void_p(llr.data_ptr()), _row_stride(llr), n, ctypes.byref(cfg), ctypes.byref(dcfg),
+            ctypes.c_void_p(out.hardbits.data_ptr()), _row_stride(out.hardbits),
             ctypes.c_void_p(out.status.data_ptr()), ctypes.c_void_p(out.iterations.data_ptr()),
             ctypes.c_void_p(out.app.data_ptr() if out.app is not None else 0),
-            out.app.stride(0) if out.app is not None else 0,
+            _row_stride(out.app) if out.app is not None else 0,
             ctypes.c_void_p(harq.data_ptr() if harq is not None else 0),
-            harq.stride(0) if harq is not None else 0,
+            _row_stride(harq) if harq is not None else 0,
             ctypes.c_void_p(stream))
     _check(rc, "nrldpc_decode_batch")
     return out
