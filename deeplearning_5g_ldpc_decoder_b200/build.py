@@ -27,6 +27,7 @@ SOURCES = [
     "nrldpc_api.cu",
     "nrldpc_fixed.cu",
     "nrldpc_float.cu",
+    "nrldpc_noalloc.cu",
     "nrldpc_tables.cpp",
 ]
 HEADERS = [

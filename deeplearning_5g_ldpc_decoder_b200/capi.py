@@ -77,6 +77,7 @@ EXPORTED_SYMBOLS = (
     "calculate_crc",
     "nrldpc_decode_batch",
     "nrldpc_decode_batch_host",
+    "nrldpc_decode_batch_noalloc",
     "nrldpc_set_trained_weights",
     "nrldpc_set_degree_alpha",
     "nrldpc_kernel_launch_count",
@@ -118,6 +119,9 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nrldpc_decode_batch.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig), ctypes.POINTER(DecoderConfig),
                                         vp, i64, vp, vp, vp, i64, vp, i64, vp]
     lib.nrldpc_decode_batch.restype = i32
+    lib.nrldpc_decode_batch_noalloc.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig),
+                                                ctypes.POINTER(DecoderConfig), vp, i64, vp, vp, vp, i64, vp, i64, vp]
+    lib.nrldpc_decode_batch_noalloc.restype = i32
     lib.nrldpc_decode_batch_host.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig),
                                              ctypes.POINTER(DecoderConfig), vp, i64, vp, vp, vp]
     lib.nrldpc_decode_batch_host.restype = i32

@@ -368,6 +368,20 @@ int32_t decode_one(int16_t* LLr, uint8_t* hardbits, ldpc_in_config_t* inconfig, 
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+// Read-only views of the algo-2 / algo-3 tables for other translation units.
+int16_t current_degree_alpha(int deg) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  return degree_alpha(deg);
+}
+
+uint64_t current_trained_table(int bgn, std::vector<uint32_t>* ab, int* T) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  TrainedTable& t = trained(bgn);
+  *ab = t.ab;
+  *T = t.T;
+  return t.generation;
+}
+
 }  // namespace nrldpc
 
 using namespace nrldpc;

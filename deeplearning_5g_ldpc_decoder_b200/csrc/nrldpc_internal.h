@@ -3,6 +3,8 @@
 
 #include <stdint.h>
 
+#include <vector>
+
 #include "nrldpc_b200.h"
 
 namespace nrldpc {
@@ -101,5 +103,10 @@ int occupancy_float_minsum(int block, int smem);
 int occupancy_float_bp(int block, int smem);
 
 void count_launch();
+
+// Current algo-3 degree table entry and algo-2 table (copy); the latter
+// returns a generation number that changes whenever the table is replaced.
+int16_t current_degree_alpha(int deg);
+uint64_t current_trained_table(int bgn, std::vector<uint32_t>* ab, int* T);
 
 }  // namespace nrldpc

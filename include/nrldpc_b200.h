@@ -163,6 +163,29 @@ int32_t nrldpc_decode_batch_host(const int16_t *h_llr, int64_t llr_stride,
                                  int32_t *h_status, int32_t *h_iterations,
                                  void *stream);
 
+/* No counterpart in the reference.  The fixed-point decode (algos 1-3) of
+ * nrldpc_decode_batch, same arguments and results, for callers that may not
+ * allocate device memory: real-time receive pipelines that cannot afford
+ * cudaMalloc's device synchronisation and latency mid-slot, and host
+ * frameworks that own every device allocation.  It calls no cudaMalloc /
+ * cudaFree: its message scratch (32 MiB, bounding the CTAs in flight) and
+ * tables are static device arrays of the library, held by every GPU that uses
+ * this entry point until the process exits.  The first call on a device
+ * resolves those arrays and uploads the CRC table, so make it before any
+ * stream capture.  All calls share the arrays: calls that overlap on the GPU
+ * race and must be serialised by the caller.  Returns -3 for algos 0 and 4,
+ * -4 if an algo-2 table has more than 64 iterations or a configuration needs
+ * more scratch per CTA than the array holds. */
+int32_t nrldpc_decode_batch_noalloc(const int16_t *d_llr, int64_t llr_stride,
+                                    int32_t num_cw,
+                                    const ldpc_in_config_t *inconfig,
+                                    const ldpc_decoder_cfg_t *decoder_cfg,
+                                    uint8_t *d_hardbits, int64_t bits_stride,
+                                    int32_t *d_status, int32_t *d_iterations,
+                                    void *d_app, int64_t app_stride,
+                                    int16_t *d_harq, int64_t harq_stride,
+                                    void *stream);
+
 /* Replace the per-(iteration, row) alpha/beta tables used by algo 2 for one
  * base graph (the reference compiles these in:
  * c_lib/BG1_trained_ldpc_weights.c:34,171, c_lib/BG2_trained_ldpc_weights.c).
