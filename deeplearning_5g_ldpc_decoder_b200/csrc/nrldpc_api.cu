@@ -190,6 +190,7 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
     const uint32_t colbase = (uint32_t)g.col[e] * (uint32_t)cp.Zc;
     const uint32_t sh = (uint32_t)(g.vij[cp.iLS][e] % cp.Zc);
     p.edge[e] = colbase | (sh << 16);
+    p.edge_cs4[e] = make_uint2(4u * colbase, 4u * sh);
   }
   for (int r = 0; r <= g.rows; ++r) p.row_off[r] = g.row_off[r];
 
@@ -237,7 +238,8 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
     } else {
       planes = 4;
     }
-    off += (uint32_t)planes * (uint32_t)p.nact;
+    // The fixed-point kernel addresses its planes with a compile-time stride.
+    off += (uint32_t)planes * (uint32_t)(fixed ? kThreadsTarget : p.nact);
   }
   p.lr_off[g.rows] = off;
   p.scratch_words = off;

@@ -5,6 +5,8 @@
 
 #include <vector>
 
+#include <vector_types.h>
+
 #include "nrldpc_b200.h"
 
 namespace nrldpc {
@@ -86,6 +88,9 @@ struct DecodeParams {
   int64_t scratch_words;   // per CTA
   // Per edge: (base column * Zc) in the low 16 bits, (V_ij mod Zc) in the high.
   uint32_t edge[kMaxNnz];
+  // The same two fields as byte offsets of 32-bit shared-memory words
+  // {base column * Zc * 4, (V_ij mod Zc) * 4}, used by the fixed-point kernel.
+  uint2 edge_cs4[kMaxNnz];
   uint32_t lr_off[kMaxRows + 1];   // per-layer word offset inside a CTA's scratch
   uint32_t w_inline[kMaxRows];
   uint16_t row_off[kMaxRows + 1];

@@ -131,8 +131,12 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
   p.max_llr = dc->max_llr;
   p.min_llr = dc->min_llr;
   p.crc_tab = nd->crc + (size_t)cp.crctype * kMaxB;
-  for (int e = 0; e < g.nnz; ++e)
-    p.edge[e] = ((uint32_t)g.col[e] * (uint32_t)cp.Zc) | ((uint32_t)(g.vij[cp.iLS][e] % cp.Zc) << 16);
+  for (int e = 0; e < g.nnz; ++e) {
+    const uint32_t colbase = (uint32_t)g.col[e] * (uint32_t)cp.Zc;
+    const uint32_t sh = (uint32_t)(g.vij[cp.iLS][e] % cp.Zc);
+    p.edge[e] = colbase | (sh << 16);
+    p.edge_cs4[e] = make_uint2(4u * colbase, 4u * sh);
+  }
   for (int r = 0; r <= g.rows; ++r) p.row_off[r] = g.row_off[r];
   p.G = std::max(1, kThreadsTarget / cp.Zc);
   p.nact = p.G * cp.Zc;
@@ -167,7 +171,7 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
   uint32_t off = 0;
   for (int r = 0; r < g.rows; ++r) {
     p.lr_off[r] = off;
-    off += (uint32_t)(g.degree[r] > 16 ? 5 : 4) * (uint32_t)p.nact;
+    off += (uint32_t)(g.degree[r] > 16 ? 5 : 4) * (uint32_t)kThreadsTarget;
   }
   p.lr_off[g.rows] = off;
   p.scratch_words = off;
