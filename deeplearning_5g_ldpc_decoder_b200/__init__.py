@@ -20,12 +20,13 @@ __all__ = [
     "make_in_config",
     "ldpc_decode",
     "ldpc_decode_host",
+    "ldpc_encode",
 ]
 
 
 def __getattr__(name):
     # torch is imported lazily so the ctypes layer works without it.
-    if name in ("ldpc_decode", "ldpc_decode_host", "code_params", "set_trained_weights", "set_degree_alpha",
+    if name in ("ldpc_decode", "ldpc_decode_host", "ldpc_encode", "code_params", "set_trained_weights", "set_degree_alpha",
                 "DecodeResult"):
         from . import decoder
 

@@ -74,7 +74,10 @@ EXPORTED_SYMBOLS = (
     "gen_ldpc_parameters",
     "cuda_ldpc_5g_decode",
     "c_ldpc_5g_decode",
+    "cuda_ldpc_5g_encode",
+    "c_ldpc_5g_encode",
     "calculate_crc",
+    "nrldpc_encode_batch",
     "nrldpc_decode_batch",
     "nrldpc_decode_batch_host",
     "nrldpc_decode_batch_noalloc",
@@ -114,6 +117,12 @@ def _declare(lib: ctypes.CDLL) -> None:
         f = getattr(lib, name)
         f.argtypes = [vp, vp, ctypes.POINTER(LdpcInConfig), ctypes.POINTER(DecoderConfig)]
         f.restype = i32
+    for name in ("cuda_ldpc_5g_encode", "c_ldpc_5g_encode"):
+        f = getattr(lib, name)
+        f.argtypes = [vp, vp, ctypes.POINTER(LdpcInConfig)]
+        f.restype = i32
+    lib.nrldpc_encode_batch.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig), vp, i64, vp]
+    lib.nrldpc_encode_batch.restype = i32
     lib.calculate_crc.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.calculate_crc.restype = ctypes.c_uint32
     lib.nrldpc_decode_batch.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig), ctypes.POINTER(DecoderConfig),

@@ -101,6 +101,7 @@ struct DeviceState {
   // single-code-block ABI
   int16_t* harq = nullptr;          // [68*384] int16, process-wide soft buffer
   Buffer one_llr, one_bits, one_stat;
+  Buffer one_info, one_rm;            // single-code-block encoder staging
   cudaStream_t one_stream = nullptr;
   // host-buffer batched API
   struct HostStage {
@@ -366,6 +367,66 @@ int32_t decode_one(int16_t* LLr, uint8_t* hardbits, ldpc_in_config_t* inconfig, 
   return status;
 }
 
+// Launch parameters of the batched encoder for one configuration.
+void make_encode_params(const CodeParams& cp, DeviceState* st, EncodeParams* e) {
+  memset(e, 0, sizeof(*e));
+  const BaseGraph& g = base_graph(cp.bgn);
+  e->bgn = cp.bgn;
+  e->Zc = cp.Zc;
+  e->R = g.rows;
+  e->cols = g.cols;
+  e->A = cp.A;
+  e->B = cp.B;
+  e->K = cp.K;
+  e->F = cp.F;
+  e->N = cp.N;
+  e->Nv = cp.Nv;
+  e->E = cp.E;
+  e->Qm = cp.Qm;
+  e->symbols = cp.symbols;
+  e->c0 = cp.c0;
+  e->Kb = cp.K / cp.Zc;
+  for (int i = 0; i < g.nnz; ++i) e->edge[i] = (uint32_t)g.col[i] | ((uint32_t)(g.vij[cp.iLS][i] % cp.Zc) << 16);
+  for (int r = 0; r <= g.rows; ++r) e->row_off[r] = g.row_off[r];
+  // Core parity circulants (c_lib/ldpc_encoder.c:95-109): BG1 row 0 / row 1 at
+  // base column 22, BG2 row 0 / row 2 at base column 10.
+  if (cp.bgn == 1) {
+    e->shift0 = g.vij[cp.iLS][g.row_off[0] + 17] % cp.Zc;
+    e->shift1 = g.vij[cp.iLS][g.row_off[1] + 16] % cp.Zc;
+  } else {
+    e->shift0 = g.vij[cp.iLS][g.row_off[0] + 6] % cp.Zc;
+    e->shift1 = g.vij[cp.iLS][g.row_off[2] + 5] % cp.Zc;
+  }
+  e->crc_tab = st->crc_tab + (size_t)cp.crctype * kMaxB;
+}
+
+int32_t encode_one(uint8_t* infobytes, uint8_t* rm_bytes, ldpc_in_config_t* inconfig) {
+  if (!inconfig) return NRLDPC_ERR_CONFIG;
+  CodeParams cp;
+  if (derive_params(*inconfig, &cp, true) != 0) return NRLDPC_ERR_CONFIG;
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
+  const int in_bytes = std::max(cp.A / 8, 1), out_bytes = std::max((cp.E + 7) / 8, 1);
+  if ((cp.A > 0 && !infobytes) || (cp.E > 0 && !rm_bytes)) return NRLDPC_ERR_CUDA;
+  if (ensure(&st->one_info, (size_t)in_bytes) || ensure(&st->one_rm, (size_t)out_bytes)) return NRLDPC_ERR_CUDA;
+  cudaStream_t s = st->one_stream;
+  if (cp.A > 0 && cudaMemcpyAsync(st->one_info.ptr, infobytes, cp.A / 8, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  EncodeParams e;
+  make_encode_params(cp, st, &e);
+  e.num_cw = 1;
+  e.info = static_cast<const uint8_t*>(st->one_info.ptr);
+  e.info_stride = in_bytes;
+  e.rm = static_cast<uint8_t*>(st->one_rm.ptr);
+  e.rm_stride = out_bytes;
+  if (launch_encode(e, s) != 0) return NRLDPC_ERR_CUDA;
+  if (cp.E > 0 && cudaMemcpyAsync(rm_bytes, st->one_rm.ptr, (cp.E + 7) / 8, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return NRLDPC_ERR_CUDA;
+  return NRLDPC_OK;
+}
+
 }  // namespace
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -508,5 +569,33 @@ int32_t nrldpc_set_degree_alpha(const int16_t* degree_alpha_values) {
 int64_t nrldpc_kernel_launch_count(void) { return g_launches.load(); }
 
 const char* nrldpc_version(void) { return "nrldpc-b200 0.1.0 (sm_100a)"; }
+
+int32_t nrldpc_encode_batch(const uint8_t* d_info, int64_t info_stride, int32_t num_cw,
+                            const ldpc_in_config_t* inconfig, uint8_t* d_rm, int64_t rm_stride, void* stream) {
+  if (!inconfig || num_cw < 0) return NRLDPC_ERR_ARG;
+  CodeParams cp;
+  if (derive_params(*inconfig, &cp, true) != 0) return NRLDPC_ERR_CONFIG;
+  if (num_cw == 0) return NRLDPC_OK;
+  if (!d_info || !d_rm || info_stride < cp.A / 8 || rm_stride < (cp.E + 7) / 8) return NRLDPC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
+  EncodeParams e;
+  make_encode_params(cp, st, &e);
+  e.num_cw = num_cw;
+  e.info = d_info;
+  e.info_stride = info_stride;
+  e.rm = d_rm;
+  e.rm_stride = rm_stride;
+  return launch_encode(e, stream) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
+}
+
+int32_t cuda_ldpc_5g_encode(uint8_t* infobytes, uint8_t* rm_bytes, ldpc_in_config_t* inconfig) {
+  return encode_one(infobytes, rm_bytes, inconfig);
+}
+
+int32_t c_ldpc_5g_encode(uint8_t* infobytes, uint8_t* rm_bytes, ldpc_in_config_t* inconfig) {
+  return encode_one(infobytes, rm_bytes, inconfig);
+}
 
 }  // extern "C"

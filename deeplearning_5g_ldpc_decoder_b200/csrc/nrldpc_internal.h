@@ -96,7 +96,22 @@ struct DecodeParams {
   uint16_t row_off[kMaxRows + 1];
 };
 
+// Launch parameters of the batched encoder (one CTA per code block).
+struct EncodeParams {
+  int32_t bgn, Zc, R, cols, A, B, K, F, N, Nv, E, Qm, symbols, c0, Kb;
+  int32_t shift0, shift1;   // core-parity circulant shifts (mod Zc): I1/I3 and I2/I4
+  int32_t num_cw;
+  const uint32_t* crc_tab;  // T[d] of the CRC type
+  const uint8_t* info;      // [num_cw][info_stride] payload bytes (A/8 used)
+  int64_t info_stride;
+  uint8_t* rm;              // [num_cw][rm_stride] rate-matched bytes (ceil(E/8) written)
+  int64_t rm_stride;
+  uint32_t edge[kMaxNnz];   // base column in the low 16 bits, V_ij mod Zc in the high
+  uint16_t row_off[kMaxRows + 1];
+};
+
 // Kernel launchers (defined in the .cu files).  Return a cudaError_t value.
+int launch_encode(const EncodeParams& p, void* stream);
 int launch_fixed(const DecodeParams& p, int grid, int block, int smem, bool degen_clip,
                  void* stream);
 int launch_float_minsum(const DecodeParams& p, int grid, int block, int smem, void* stream);

@@ -109,6 +109,25 @@ def ldpc_decode(llr: torch.Tensor, inconfig, decoder_config, *, return_app: bool
     return out
 
 
+def ldpc_encode(info: torch.Tensor, inconfig) -> torch.Tensor:
+    """Encode a batch of payloads (uint8 CUDA tensor [n, >= A/8], MSB first) into
+    rate-matched bits packed MSB first: uint8 [n, ceil(E/8)]."""
+    cfg = _as_in_config(inconfig)
+    if not info.is_cuda or info.dtype != torch.uint8 or info.dim() != 2:
+        raise ValueError("info must be a uint8 CUDA tensor of shape [n, A/8]")
+    if info.stride(1) != 1:
+        info = info.contiguous()
+    n = info.shape[0]
+    out = torch.zeros((n, (cfg.E + 7) // 8), dtype=torch.uint8, device=info.device)
+    lib = capi.load_library()
+    stream = torch.cuda.current_stream(info.device).cuda_stream
+    with torch.cuda.device(info.device):
+        rc = lib.nrldpc_encode_batch(ctypes.c_void_p(info.data_ptr()), _row_stride(info), n, ctypes.byref(cfg),
+                                     ctypes.c_void_p(out.data_ptr()), _row_stride(out), ctypes.c_void_p(stream))
+    _check(rc, "nrldpc_encode_batch")
+    return out
+
+
 def ldpc_decode_host(llr, inconfig, decoder_config):
     """Decode from host (numpy / CPU tensor) LLRs through the host-buffer C ABI;
     returns numpy (hardbits, status, iterations)."""

@@ -114,6 +114,20 @@ int32_t c_ldpc_5g_decode(int16_t *LLr, uint8_t *hardbits,
                          ldpc_in_config_t *inconfig,
                          ldpc_decoder_cfg_t *decoder_config);
 
+/* Encode one code block from host memory: CRC attach, QC-LDPC encoding, rate
+ * matching to E bits with the Qm interleave, packed MSB first into
+ * ceil(E/8) bytes of rm_bytes.  Runs on the GPU.  Returns 0, -2 (invalid
+ * configuration) or -1 (CUDA error).  Replaces cuda_ldpc_5g_encode
+ * (CUDA/cuda_ldpc_5g_encoder.cu:47-84), the symbol the reference's BLER
+ * harness binds next to the decoder (scripts/ldpc_c_sim_common.py:76-83). */
+int32_t cuda_ldpc_5g_encode(uint8_t *infobytes, uint8_t *rm_bytes,
+                            ldpc_in_config_t *inconfig);
+
+/* Same call under the C library's symbol name (c_lib/nr_ldpc.h:129,
+ * c_lib/c_ldpc_5g_encoder.c:66-88); it runs on the GPU as well. */
+int32_t c_ldpc_5g_encode(uint8_t *infobytes, uint8_t *rm_bytes,
+                         ldpc_in_config_t *inconfig);
+
 /* Table-driven NR CRC remainder over len bytes, MSB first; 0 for an
  * unknown crctype.  Host function.  Replaces calculate_crc
  * (c_lib/nr_ldpc.h:102, c_lib/nr_crc.c:170-179). */
@@ -185,6 +199,15 @@ int32_t nrldpc_decode_batch_noalloc(const int16_t *d_llr, int64_t llr_stride,
                                     void *d_app, int64_t app_stride,
                                     int16_t *d_harq, int64_t harq_stride,
                                     void *stream);
+
+/* Encode num_cw code blocks of one configuration on the device:
+ *   d_info  uint8 [num_cw][info_stride], A/8 payload bytes used
+ *   d_rm    uint8 [num_cw][rm_stride], ceil(E/8) rate-matched bytes written
+ * Stream-ordered.  No counterpart in the reference (one block per call there).
+ * Returns 0, -1, -2 or -4. */
+int32_t nrldpc_encode_batch(const uint8_t *d_info, int64_t info_stride,
+                            int32_t num_cw, const ldpc_in_config_t *inconfig,
+                            uint8_t *d_rm, int64_t rm_stride, void *stream);
 
 /* Replace the per-(iteration, row) alpha/beta tables used by algo 2 for one
  * base graph (the reference compiles these in:
