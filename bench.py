@@ -45,6 +45,7 @@ ZC = 384
 NNZ = 316
 E = 25344
 EBN0_DB = 0.9
+ESN0_1E2_DB = 11.0   # 256QAM Es/N0 of ~1e-2 BLER for this code, algo 1, 8 iterations (measured)
 WORKLOAD = ("BG1 Zc=384 A=8424 B=8448 E=25344 (Qm=8 length, R=1/3), algo 1 int16 layered min-sum "
             "alpha=22936, 8 iterations (CRC never passes: all 8 run), 8192 code blocks per launch")
 
@@ -243,6 +244,12 @@ def run_gpu(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_step = float(t.item())
 
+    # ---- realistic inputs: device-encoded code blocks through the 256QAM channel
+    # near the 1e-2 BLER point; CRC early termination as in the reference ----
+    early = None
+    if not args.no_e2e:
+        early = run_early_exit(args, n_cw, dev, stream, barrier, dist, torch)
+
     # ---- end to end through the host-buffer C ABI (pinned memory) ----
     if args.no_e2e:
         e2e_ms = float("nan")
@@ -288,6 +295,7 @@ def run_gpu(args, rank, world, local_rank):
                          "io_bytes_per_launch": float((2 * E + (B_BITS + 7) // 8 + 4) * n_cw)},
             "iterations_executed_mean": float(np.mean(iters)),
             "converged": int(np.sum(status == 0)),
+            "early_exit": early,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
@@ -297,6 +305,38 @@ def run_gpu(args, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+def run_early_exit(args, n_cw, dev, stream, barrier, dist, torch):
+    from deeplearning_5g_ldpc_decoder_b200 import channel_llrs, ldpc_decode, ldpc_encode
+
+    gen = torch.Generator(device=dev).manual_seed(1234)
+    pay = torch.randint(0, 256, (n_cw, A_BITS // 8), dtype=torch.uint8, device=dev, generator=gen)
+    llr = channel_llrs(ldpc_encode(pay, CFG), E, 8, noise_power_db=-ESN0_1E2_DB, seed=99)
+    out = None
+    for _ in range(max(args.warmup, 1)):
+        out = ldpc_decode(llr, CFG, ROW, out=out)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        out = ldpc_decode(llr, CFG, ROW, out=out)
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ok = (out.status == 0) & (out.hardbits[:, : A_BITS // 8] == pay).all(dim=1)
+    iters = out.iterations.cpu().numpy()
+    world = dist.get_world_size() if dist is not None else 1
+    return {"value": round(n_cw * A_BITS * world / (ms * 1e-3) / 1e9, 4), "unit": "Gbit/s", "ms_per_step": round(ms, 4),
+            "iterations_executed_mean": float(np.mean(iters)), "bler": float(1.0 - ok.float().mean().item()),
+            "roofline_achieved_gbs": round(algorithmic_bytes(iters) / (ms * 1e-3) / 1e9, 1),
+            "inputs": f"device-encoded random payloads, 256QAM AWGN at Es/N0 {ESN0_1E2_DB} dB, max-log LLRs "
+                      "quantised like the reference channel"}
 
 
 def run_e2e(args, lib, host_llr, out, stream, barrier, dist, dev, iters, torch):

@@ -21,12 +21,13 @@ __all__ = [
     "ldpc_decode",
     "ldpc_decode_host",
     "ldpc_encode",
+    "channel_llrs",
 ]
 
 
 def __getattr__(name):
     # torch is imported lazily so the ctypes layer works without it.
-    if name in ("ldpc_decode", "ldpc_decode_host", "ldpc_encode", "code_params", "set_trained_weights", "set_degree_alpha",
+    if name in ("ldpc_decode", "ldpc_decode_host", "ldpc_encode", "channel_llrs", "code_params", "set_trained_weights", "set_degree_alpha",
                 "DecodeResult"):
         from . import decoder
 

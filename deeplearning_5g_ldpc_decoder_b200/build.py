@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
 
 SOURCES = [
     "nrldpc_api.cu",
+    "nrldpc_channel.cu",
     "nrldpc_encode.cu",
     "nrldpc_fixed.cu",
     "nrldpc_float.cu",

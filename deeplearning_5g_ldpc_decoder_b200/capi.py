@@ -77,7 +77,10 @@ EXPORTED_SYMBOLS = (
     "cuda_ldpc_5g_encode",
     "c_ldpc_5g_encode",
     "calculate_crc",
+    "tx_rx_process",
     "nrldpc_encode_batch",
+    "nrldpc_channel_batch",
+    "nrldpc_channel_seed",
     "nrldpc_decode_batch",
     "nrldpc_decode_batch_host",
     "nrldpc_decode_batch_noalloc",
@@ -122,6 +125,12 @@ def _declare(lib: ctypes.CDLL) -> None:
         f.argtypes = [vp, vp, ctypes.POINTER(LdpcInConfig)]
         f.restype = i32
     lib.nrldpc_encode_batch.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig), vp, i64, vp]
+    lib.nrldpc_channel_batch.argtypes = [vp, i64, i32, i32, i32, ctypes.c_float, ctypes.c_uint64, vp, i64, vp, vp]
+    lib.nrldpc_channel_batch.restype = i32
+    lib.nrldpc_channel_seed.argtypes = [ctypes.c_uint64]
+    lib.nrldpc_channel_seed.restype = None
+    lib.tx_rx_process.argtypes = [vp, ctypes.c_size_t, ctypes.c_uint16, ctypes.c_float, vp]
+    lib.tx_rx_process.restype = ctypes.c_int
     lib.nrldpc_encode_batch.restype = i32
     lib.calculate_crc.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.calculate_crc.restype = ctypes.c_uint32

@@ -12,11 +12,34 @@
 #include <utility>
 #include <vector>
 
+#include <math.h>
+
 #include "nrldpc_internal.h"
 
 namespace nrldpc {
 
 namespace {
+
+uint64_t g_channel_seed = 0x5EEDull;
+uint64_t g_channel_calls = 0;
+
+// Channel constants exactly as the reference computes them in float
+// (c_lib/tx_rx_process.c:71-97, :298-299).
+bool channel_constants(int Qm, float noise_power_db, float* nv, float* sigma, float* A) {
+  float k;
+  switch (Qm) {
+    case 1:
+    case 2: k = 2.0f; break;
+    case 4: k = 10.0f; break;
+    case 6: k = 42.0f; break;
+    case 8: k = 170.0f; break;
+    default: return false;
+  }
+  *A = 1.0f / sqrtf(k);
+  *nv = powf(10.0f, noise_power_db / 10.0f);
+  *sigma = sqrtf(*nv / 2.0f);
+  return true;
+}
 
 std::atomic<int64_t> g_launches{0};
 std::mutex g_mu;
@@ -102,6 +125,7 @@ struct DeviceState {
   int16_t* harq = nullptr;          // [68*384] int16, process-wide soft buffer
   Buffer one_llr, one_bits, one_stat;
   Buffer one_info, one_rm;            // single-code-block encoder staging
+  Buffer ch_in, ch_out;               // host-buffer channel staging
   cudaStream_t one_stream = nullptr;
   // host-buffer batched API
   struct HostStage {
@@ -596,6 +620,45 @@ int32_t cuda_ldpc_5g_encode(uint8_t* infobytes, uint8_t* rm_bytes, ldpc_in_confi
 
 int32_t c_ldpc_5g_encode(uint8_t* infobytes, uint8_t* rm_bytes, ldpc_in_config_t* inconfig) {
   return encode_one(infobytes, rm_bytes, inconfig);
+}
+
+int32_t nrldpc_channel_batch(const uint8_t* d_rm, int64_t rm_stride, int32_t num_cw, int32_t E, int32_t Qm,
+                             float noise_power_db, uint64_t seed, int16_t* d_llr, int64_t llr_stride,
+                             float* d_symbols, void* stream) {
+  float nv, sigma, A;
+  if (num_cw < 0 || E < 0 || !channel_constants(Qm, noise_power_db, &nv, &sigma, &A) || E % Qm) return NRLDPC_ERR_ARG;
+  if (num_cw == 0 || E == 0) return NRLDPC_OK;
+  if (!d_rm || !d_llr || rm_stride < (E + 7) / 8 || llr_stride < E) return NRLDPC_ERR_ARG;
+  return launch_channel(d_rm, rm_stride, num_cw, E, Qm, nv, sigma, A, seed, d_llr, llr_stride, d_symbols, stream) == 0
+             ? NRLDPC_OK
+             : NRLDPC_ERR_CUDA;
+}
+
+void nrldpc_channel_seed(uint64_t seed) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  g_channel_seed = seed;
+  g_channel_calls = 0;
+}
+
+int tx_rx_process(const uint8_t* inbytes, size_t num_bits, uint16_t Qm, float noise_power_db, int16_t* llr_out) {
+  float nv, sigma, A;
+  if (!inbytes || !llr_out || num_bits == 0) return -1;
+  if (!channel_constants(Qm, noise_power_db, &nv, &sigma, &A) || num_bits % Qm) return -1;
+  if (num_bits > (size_t)INT32_MAX) return -1;
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return -1;
+  const size_t in_bytes = (num_bits + 7) / 8;
+  if (ensure(&st->ch_in, in_bytes) || ensure(&st->ch_out, num_bits * sizeof(int16_t))) return -1;
+  cudaStream_t s = st->one_stream;
+  const uint64_t seed = g_channel_seed ^ (0x9E3779B97F4A7C15ull * ++g_channel_calls);
+  if (cudaMemcpyAsync(st->ch_in.ptr, inbytes, in_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return -1;
+  if (launch_channel(static_cast<uint8_t*>(st->ch_in.ptr), (int64_t)in_bytes, 1, (int32_t)num_bits, Qm, nv, sigma, A,
+                     seed, static_cast<int16_t*>(st->ch_out.ptr), (int64_t)num_bits, nullptr, s) != 0)
+    return -1;
+  if (cudaMemcpyAsync(llr_out, st->ch_out.ptr, num_bits * sizeof(int16_t), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return -1;
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -1;
 }
 
 }  // extern "C"

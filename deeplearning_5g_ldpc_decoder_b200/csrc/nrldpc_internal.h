@@ -112,6 +112,9 @@ struct EncodeParams {
 
 // Kernel launchers (defined in the .cu files).  Return a cudaError_t value.
 int launch_encode(const EncodeParams& p, void* stream);
+int launch_channel(const uint8_t* rm, int64_t rm_stride, int32_t num_cw, int32_t E, int32_t Qm, float nv,
+                   float sigma, float A, uint64_t seed, int16_t* llr, int64_t llr_stride, float* symbols,
+                   void* stream);
 int launch_fixed(const DecodeParams& p, int grid, int block, int smem, bool degen_clip,
                  void* stream);
 int launch_float_minsum(const DecodeParams& p, int grid, int block, int smem, void* stream);

@@ -128,6 +128,31 @@ def ldpc_encode(info: torch.Tensor, inconfig) -> torch.Tensor:
     return out
 
 
+def channel_llrs(rm: torch.Tensor, E: int, Qm: int, noise_power_db: float, seed: int = 0,
+                 return_symbols: bool = False):
+    """Device LLR front-end: packed rate-matched bits (uint8 CUDA [n, ceil(E/8)])
+    -> NR QAM -> AWGN (power 10^(noise_power_db/10)) -> max-log LLRs quantised
+    to int16 like the reference channel.  Returns int16 [n, E] (and the noisy
+    symbols float [n, E/Qm, 2] when asked)."""
+    if not rm.is_cuda or rm.dtype != torch.uint8 or rm.dim() != 2:
+        raise ValueError("rm must be a uint8 CUDA tensor [n, ceil(E/8)]")
+    if rm.stride(1) != 1:
+        rm = rm.contiguous()
+    n = rm.shape[0]
+    llr = torch.empty((n, E), dtype=torch.int16, device=rm.device)
+    sym = torch.empty((n, E // Qm, 2), dtype=torch.float32, device=rm.device) if return_symbols else None
+    lib = capi.load_library()
+    stream = torch.cuda.current_stream(rm.device).cuda_stream
+    with torch.cuda.device(rm.device):
+        rc = lib.nrldpc_channel_batch(ctypes.c_void_p(rm.data_ptr()), _row_stride(rm), n, E, Qm,
+                                      ctypes.c_float(noise_power_db), ctypes.c_uint64(seed),
+                                      ctypes.c_void_p(llr.data_ptr()), E,
+                                      ctypes.c_void_p(sym.data_ptr() if sym is not None else 0),
+                                      ctypes.c_void_p(stream))
+    _check(rc, "nrldpc_channel_batch")
+    return (llr, sym) if return_symbols else llr
+
+
 def ldpc_decode_host(llr, inconfig, decoder_config):
     """Decode from host (numpy / CPU tensor) LLRs through the host-buffer C ABI;
     returns numpy (hardbits, status, iterations)."""

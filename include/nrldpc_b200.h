@@ -128,6 +128,16 @@ int32_t cuda_ldpc_5g_encode(uint8_t *infobytes, uint8_t *rm_bytes,
 int32_t c_ldpc_5g_encode(uint8_t *infobytes, uint8_t *rm_bytes,
                          ldpc_in_config_t *inconfig);
 
+/* Test channel: unpack num_bits MSB-first bits, NR QAM-map them (Qm 1..8),
+ * add complex AWGN of power 10^(noise_power_db/10), max-log demap and
+ * quantise round(128*LLR) to +-10000.  Runs on the GPU from host buffers.
+ * Same signature, arguments and return codes (0 / -1) as the reference's
+ * tx_rx_process (c_lib/nr_ldpc.h:123, c_lib/tx_rx_process.c:286-324); the
+ * noise comes from this library's own generator, seeded by
+ * nrldpc_channel_seed() instead of srand(). */
+int tx_rx_process(const uint8_t *inbytes, size_t num_bits, uint16_t Qm,
+                  float noise_power_db, int16_t *llr_out);
+
 /* Table-driven NR CRC remainder over len bytes, MSB first; 0 for an
  * unknown crctype.  Host function.  Replaces calculate_crc
  * (c_lib/nr_ldpc.h:102, c_lib/nr_crc.c:170-179). */
@@ -208,6 +218,21 @@ int32_t nrldpc_decode_batch_noalloc(const int16_t *d_llr, int64_t llr_stride,
 int32_t nrldpc_encode_batch(const uint8_t *d_info, int64_t info_stride,
                             int32_t num_cw, const ldpc_in_config_t *inconfig,
                             uint8_t *d_rm, int64_t rm_stride, void *stream);
+
+/* Device LLR front-end for num_cw blocks: d_rm uint8 [num_cw][rm_stride]
+ * (ceil(E/8) packed bits used) -> d_llr int16 [num_cw][llr_stride] (E
+ * values), through the same mapping / AWGN / demapping / quantisation as
+ * tx_rx_process.  The noise of (block, symbol) is a fixed function of seed.
+ * d_symbols (nullable) receives the noisy symbols, float [num_cw][E/Qm][2].
+ * Stream-ordered.  No counterpart in the reference.  Returns 0, -1 or -4. */
+int32_t nrldpc_channel_batch(const uint8_t *d_rm, int64_t rm_stride,
+                             int32_t num_cw, int32_t E, int32_t Qm,
+                             float noise_power_db, uint64_t seed,
+                             int16_t *d_llr, int64_t llr_stride,
+                             float *d_symbols, void *stream);
+
+/* Seed of tx_rx_process's noise generator (the reference uses srand()). */
+void nrldpc_channel_seed(uint64_t seed);
 
 /* Replace the per-(iteration, row) alpha/beta tables used by algo 2 for one
  * base graph (the reference compiles these in:
