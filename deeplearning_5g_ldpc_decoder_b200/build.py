@@ -29,12 +29,15 @@ SOURCES = [
     "nrldpc_encode.cu",
     "nrldpc_fixed.cu",
     "nrldpc_float.cu",
+    "nrldpc_mixed.cu",
+    "nrldpc_mixed_api.cu",
     "nrldpc_noalloc.cu",
     "nrldpc_tables.cpp",
 ]
 HEADERS = [
     "nrldpc_internal.h",
     "nrldpc_decode_common.cuh",
+    "nrldpc_fixed_row.cuh",
     "nr_base_graphs.inc",
 ]
 

@@ -455,6 +455,22 @@ int32_t encode_one(uint8_t* infobytes, uint8_t* rm_bytes, ldpc_in_config_t* inco
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+// Device tables of the current device, for other translation units.
+int device_crc_table(const uint32_t** tab) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
+  *tab = st->crc_tab;
+  return NRLDPC_OK;
+}
+
+int device_trained_table(int bgn, const uint32_t** ptr, int* T) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
+  return trained_device_table(st, bgn, ptr, T) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
+}
+
 // Read-only views of the algo-2 / algo-3 tables for other translation units.
 int16_t current_degree_alpha(int deg) {
   std::lock_guard<std::mutex> lock(g_mu);

@@ -110,8 +110,50 @@ struct EncodeParams {
   uint16_t row_off[kMaxRows + 1];
 };
 
+// ---- mixed-size batches (one persistent kernel, work queue) ----
+// Base-graph tables of one (BG, Zc), staged into shared memory per work item.
+struct MixedGraph {
+  int32_t bgn, Zc, R, lq_len, G, K, N, pad0, pad1;
+  uint32_t lr_off[kMaxRows + 1];       // scratch plane offsets, plane stride kThreadsTarget
+  uint16_t row_off[kMaxRows + 1];
+  uint16_t pad2;
+  uint2 edges[kMaxNnz];                // {col*Zc*4, (V mod Zc)*4}
+};
+// Per code block: its own rate-recovery / CRC parameters and I/O offsets.
+struct MixedCw {
+  int32_t B, E, Qm, symbols, c0, Nv, F, crctype;
+  int64_t llr_off;    // elements into the LLR arena
+  int64_t bits_off;   // bytes into the hard-bit arena
+};
+// One work item: up to G pairs of one (BG, Zc); slots[slot_base + 2g + h] = block or -1.
+struct MixedItem {
+  int32_t graph, slot_base, npairs, bmax_pad;
+};
+struct MixedParams {
+  const MixedGraph* graphs;
+  const MixedItem* items;
+  const int32_t* slots;
+  const MixedCw* cws;
+  int32_t num_items;
+  int32_t* counter;                    // work-queue head, zeroed before each launch
+  const int16_t* llr;
+  uint8_t* bits;
+  int32_t* status;
+  int32_t* iters;
+  const uint32_t* crc_tab;             // [4][kMaxB]
+  uint32_t* scratch;
+  int64_t scratch_words;               // per CTA
+  int32_t max_it, fill, max_llr, min_llr;
+  uint32_t w_inline[2][kMaxRows];      // alpha|beta<<16 per row, per base graph (algos 1, 3)
+  const uint32_t* weights[2];          // algo 2 tables per base graph
+  int32_t weights_T[2];
+};
+
 // Kernel launchers (defined in the .cu files).  Return a cudaError_t value.
 int launch_encode(const EncodeParams& p, void* stream);
+int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream);
+int prepare_mixed(bool degen_clip);
+int occupancy_mixed(bool degen_clip);
 int launch_channel(const uint8_t* rm, int64_t rm_stride, int32_t num_cw, int32_t E, int32_t Qm, float nv,
                    float sigma, float A, uint64_t seed, int16_t* llr, int64_t llr_stride, float* symbols,
                    void* stream);
@@ -130,6 +172,8 @@ void count_launch();
 // Current algo-3 degree table entry and algo-2 table (copy); the latter
 // returns a generation number that changes whenever the table is replaced.
 int16_t current_degree_alpha(int deg);
+int device_crc_table(const uint32_t** tab);
+int device_trained_table(int bgn, const uint32_t** ptr, int* T);
 uint64_t current_trained_table(int bgn, std::vector<uint32_t>* ab, int* T);
 
 }  // namespace nrldpc

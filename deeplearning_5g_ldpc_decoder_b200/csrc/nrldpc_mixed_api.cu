@@ -1,0 +1,343 @@
+// nrldpc_mixed_api.cu — host side of mixed-size batches: the plan (pairing of
+// blocks of one (BG, Zc), work items, device tables), its CUDA graph, and a
+// small autotuner over the launch shape and the work-item order.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <utility>
+#include <vector>
+
+#include "nrldpc_internal.h"
+
+namespace nrldpc {
+namespace {
+
+struct MixedPlanImpl {
+  int device = 0;
+  int num_cw = 0;
+  int num_sms = 0;
+  bool degen = false;
+  std::vector<MixedGraph> graphs;
+  std::vector<std::vector<int>> members;   // block indices per graph, in pairing order
+  std::vector<MixedCw> cws;
+  MixedGraph* d_graphs = nullptr;
+  MixedCw* d_cws = nullptr;
+  MixedItem* d_items = nullptr;
+  int32_t* d_slots = nullptr;
+  int32_t* d_counter = nullptr;
+  uint32_t* d_scratch = nullptr;
+  size_t items_cap = 0, slots_cap = 0;
+  int scratch_ctas = 0;
+  MixedParams params = {};
+  int order = 0;          // 0: largest work first, 1: graphs interleaved
+  int ctas_per_sm = 2;
+  int grid = 1;
+  // captured graph
+  cudaGraphExec_t exec = nullptr;
+  const void* cap_ptrs[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t cap_stream = nullptr;
+  int cap_order = -1, cap_ctas = -1;
+};
+
+constexpr uint32_t kScratchWordsPerCta = (4 * 42 + 5 * 4) * kThreadsTarget;   // BG1 layout, the larger one
+
+void free_plan(MixedPlanImpl* pl) {
+  if (pl->exec) cudaGraphExecDestroy(pl->exec);
+  cudaFree(pl->d_graphs);
+  cudaFree(pl->d_cws);
+  cudaFree(pl->d_items);
+  cudaFree(pl->d_slots);
+  cudaFree(pl->d_counter);
+  cudaFree(pl->d_scratch);
+  delete pl;
+}
+
+MixedGraph make_graph(int bgn, int Zc, int iLS) {
+  MixedGraph m;
+  memset(&m, 0, sizeof(m));
+  const BaseGraph& g = base_graph(bgn);
+  m.bgn = bgn;
+  m.Zc = Zc;
+  m.R = g.rows;
+  m.lq_len = g.cols * Zc;
+  m.G = std::max(1, kThreadsTarget / Zc);
+  m.K = (bgn == 1 ? 22 : 10) * Zc;
+  m.N = (bgn == 1 ? 66 : 50) * Zc;
+  uint32_t off = 0;
+  for (int r = 0; r < g.rows; ++r) {
+    m.lr_off[r] = off;
+    off += (uint32_t)(g.degree[r] > 16 ? 5 : 4) * kThreadsTarget;
+    m.row_off[r] = g.row_off[r];
+  }
+  m.lr_off[g.rows] = off;
+  m.row_off[g.rows] = g.row_off[g.rows];
+  for (int e = 0; e < g.nnz; ++e)
+    m.edges[e] = make_uint2(4u * (uint32_t)g.col[e] * (uint32_t)Zc, 4u * (uint32_t)(g.vij[iLS][e] % Zc));
+  return m;
+}
+
+// Work items for the current order; uploads items + slots.
+int build_items(MixedPlanImpl* pl) {
+  struct It {
+    MixedItem m;
+    double cost;
+    int graph_rank;
+  };
+  std::vector<It> items;
+  std::vector<int32_t> slots;
+  for (size_t gi = 0; gi < pl->graphs.size(); ++gi) {
+    const MixedGraph& g = pl->graphs[gi];
+    const BaseGraph& bg = base_graph(g.bgn);
+    const std::vector<int>& mem = pl->members[gi];
+    const int npairs_total = ((int)mem.size() + 1) / 2;
+    int rank = 0;
+    for (int p0 = 0; p0 < npairs_total; p0 += g.G, ++rank) {
+      It it;
+      it.m.graph = (int32_t)gi;
+      it.m.slot_base = (int32_t)slots.size();
+      it.m.npairs = std::min(g.G, npairs_total - p0);
+      int bmax = 0;
+      for (int k = 0; k < 2 * g.G; ++k) {
+        const int idx = 2 * p0 + k;
+        const bool in = k < 2 * it.m.npairs && idx < (int)mem.size();
+        const int cw = in ? mem[idx] : -1;
+        slots.push_back(cw);
+        if (cw >= 0) bmax = std::max(bmax, pl->cws[cw].B);
+      }
+      it.m.bmax_pad = (bmax + 31) & ~31;
+      it.cost = (double)bg.nnz * g.Zc * it.m.npairs;
+      it.graph_rank = rank;
+      items.push_back(it);
+    }
+  }
+  if (pl->order == 0) {
+    std::stable_sort(items.begin(), items.end(), [](const It& a, const It& b) { return a.cost > b.cost; });
+  } else {
+    std::stable_sort(items.begin(), items.end(), [](const It& a, const It& b) { return a.graph_rank < b.graph_rank; });
+  }
+  std::vector<MixedItem> host(items.size());
+  for (size_t i = 0; i < items.size(); ++i) host[i] = items[i].m;
+  if (host.size() > pl->items_cap) {
+    cudaFree(pl->d_items);
+    if (cudaMalloc(&pl->d_items, host.size() * sizeof(MixedItem)) != cudaSuccess) return NRLDPC_ERR_CUDA;
+    pl->items_cap = host.size();
+  }
+  if (slots.size() > pl->slots_cap) {
+    cudaFree(pl->d_slots);
+    if (cudaMalloc(&pl->d_slots, slots.size() * sizeof(int32_t)) != cudaSuccess) return NRLDPC_ERR_CUDA;
+    pl->slots_cap = slots.size();
+  }
+  if (cudaMemcpy(pl->d_items, host.data(), host.size() * sizeof(MixedItem), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(pl->d_slots, slots.data(), slots.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
+  pl->params.items = pl->d_items;
+  pl->params.slots = pl->d_slots;
+  pl->params.num_items = (int32_t)host.size();
+  return NRLDPC_OK;
+}
+
+int configure(MixedPlanImpl* pl, int ctas_per_sm, int order) {
+  if (order != pl->order || !pl->params.items) {
+    pl->order = order;
+    const int rc = build_items(pl);
+    if (rc != NRLDPC_OK) return rc;
+  }
+  int occ = occupancy_mixed(pl->degen);
+  if (occ < 1) occ = 1;
+  pl->ctas_per_sm = std::max(1, std::min(ctas_per_sm, occ));
+  pl->grid = std::max(1, std::min(pl->params.num_items, pl->ctas_per_sm * pl->num_sms));
+  if (pl->grid > pl->scratch_ctas) {
+    cudaFree(pl->d_scratch);
+    pl->d_scratch = nullptr;
+    if (cudaMalloc(&pl->d_scratch, (size_t)pl->grid * kScratchWordsPerCta * sizeof(uint32_t)) != cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+    pl->scratch_ctas = pl->grid;
+  }
+  pl->params.scratch = pl->d_scratch;
+  return NRLDPC_OK;
+}
+
+int enqueue(MixedPlanImpl* pl, cudaStream_t s) {
+  if (cudaMemsetAsync(pl->params.counter, 0, sizeof(int32_t), s) != cudaSuccess) return NRLDPC_ERR_CUDA;
+  return launch_mixed(pl->params, pl->grid, pl->degen, s) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
+}
+
+int execute(MixedPlanImpl* pl, const int16_t* llr, uint8_t* bits, int32_t* status, int32_t* iters, bool use_graph,
+            cudaStream_t s) {
+  pl->params.llr = llr;
+  pl->params.bits = bits;
+  pl->params.status = status;
+  pl->params.iters = iters;
+  if (!use_graph || s == nullptr) return enqueue(pl, s);
+  const void* ptrs[4] = {llr, bits, status, iters};
+  const bool same = pl->exec && s == pl->cap_stream && pl->cap_order == pl->order && pl->cap_ctas == pl->grid &&
+                    memcmp(ptrs, pl->cap_ptrs, sizeof(ptrs)) == 0;
+  if (!same) {
+    if (pl->exec) cudaGraphExecDestroy(pl->exec);
+    pl->exec = nullptr;
+    if (prepare_mixed(pl->degen) != 0) return NRLDPC_ERR_CUDA;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return NRLDPC_ERR_CUDA;
+    const int rc = enqueue(pl, s);
+    if (cudaStreamEndCapture(s, &graph) != cudaSuccess || rc != NRLDPC_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return NRLDPC_ERR_CUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&pl->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return NRLDPC_ERR_CUDA;
+    memcpy(pl->cap_ptrs, ptrs, sizeof(ptrs));
+    pl->cap_stream = s;
+    pl->cap_order = pl->order;
+    pl->cap_ctas = pl->grid;
+  }
+  if (cudaGraphLaunch(pl->exec, s) != cudaSuccess) return NRLDPC_ERR_CUDA;
+  count_launch();   // the kernel node of the replayed graph
+  return NRLDPC_OK;
+}
+
+}  // namespace
+}  // namespace nrldpc
+
+using namespace nrldpc;
+
+extern "C" {
+
+int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_blocks, const ldpc_decoder_cfg_t* dc,
+                                 void** plan_out) {
+  if (!plan_out || !dc || num_blocks <= 0 || !blocks) return NRLDPC_ERR_ARG;
+  *plan_out = nullptr;
+  if (dc->algo < 1 || dc->algo > 3) {
+    fprintf(stderr, "nrldpc_mixed_plan_create: fixed-point algos 1-3 only (got %u)\n", dc->algo);
+    return NRLDPC_ERR_ALGO;
+  }
+  MixedPlanImpl* pl = new MixedPlanImpl();
+  cudaGetDevice(&pl->device);
+  if (cudaDeviceGetAttribute(&pl->num_sms, cudaDevAttrMultiProcessorCount, pl->device) != cudaSuccess) {
+    delete pl;
+    return NRLDPC_ERR_CUDA;
+  }
+  pl->num_cw = num_blocks;
+  pl->degen = dc->min_llr > dc->max_llr;
+  std::map<std::pair<int, int>, int> gidx;
+  pl->cws.resize(num_blocks);
+  for (int i = 0; i < num_blocks; ++i) {
+    CodeParams cp;
+    if (derive_params(blocks[i].cfg, &cp, true) != 0) {
+      delete pl;
+      return NRLDPC_ERR_CONFIG;
+    }
+    if (cp.harq_on || blocks[i].llr_offset < 0 || blocks[i].bits_offset < 0) {
+      delete pl;
+      return NRLDPC_ERR_ARG;
+    }
+    const auto key = std::make_pair(cp.bgn, cp.Zc);
+    auto itg = gidx.find(key);
+    if (itg == gidx.end()) {
+      itg = gidx.emplace(key, (int)pl->graphs.size()).first;
+      pl->graphs.push_back(make_graph(cp.bgn, cp.Zc, cp.iLS));
+      pl->members.emplace_back();
+    }
+    pl->members[itg->second].push_back(i);
+    MixedCw& c = pl->cws[i];
+    c.B = cp.B;
+    c.E = cp.E;
+    c.Qm = cp.Qm;
+    c.symbols = cp.symbols;
+    c.c0 = cp.c0;
+    c.Nv = cp.Nv;
+    c.F = cp.F;
+    c.crctype = cp.crctype;
+    c.llr_off = blocks[i].llr_offset;
+    c.bits_off = blocks[i].bits_offset;
+  }
+  MixedParams& p = pl->params;
+  p.max_it = dc->max_iterations;
+  p.fill = dc->filling_bit_value;
+  p.max_llr = dc->max_llr;
+  p.min_llr = dc->min_llr;
+  p.scratch_words = kScratchWordsPerCta;
+  for (int b = 0; b < 2; ++b) {
+    const BaseGraph& g = base_graph(b + 1);
+    for (int r = 0; r < g.rows; ++r) {
+      const int16_t alpha = dc->algo == 3 ? current_degree_alpha(g.degree[r]) : (int16_t)dc->alpha;
+      p.w_inline[b][r] = pack_ab(alpha, (int16_t)dc->beta);
+    }
+    p.weights_T[b] = 0;
+    if (dc->algo == 2 && device_trained_table(b + 1, &p.weights[b], &p.weights_T[b]) != NRLDPC_OK) {
+      delete pl;
+      return NRLDPC_ERR_CUDA;
+    }
+  }
+  if (device_crc_table(&p.crc_tab) != NRLDPC_OK ||
+      cudaMalloc(&pl->d_graphs, pl->graphs.size() * sizeof(MixedGraph)) != cudaSuccess ||
+      cudaMalloc(&pl->d_cws, pl->cws.size() * sizeof(MixedCw)) != cudaSuccess ||
+      cudaMalloc(&pl->d_counter, sizeof(int32_t)) != cudaSuccess ||
+      cudaMemcpy(pl->d_graphs, pl->graphs.data(), pl->graphs.size() * sizeof(MixedGraph), cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy(pl->d_cws, pl->cws.data(), pl->cws.size() * sizeof(MixedCw), cudaMemcpyHostToDevice) !=
+          cudaSuccess) {
+    free_plan(pl);
+    return NRLDPC_ERR_CUDA;
+  }
+  p.graphs = pl->d_graphs;
+  p.cws = pl->d_cws;
+  p.counter = pl->d_counter;
+  const int rc = configure(pl, 2, 0);
+  if (rc != NRLDPC_OK) {
+    free_plan(pl);
+    return rc;
+  }
+  *plan_out = pl;
+  return NRLDPC_OK;
+}
+
+int32_t nrldpc_mixed_plan_execute(void* plan, const int16_t* d_llr, uint8_t* d_bits, int32_t* d_status,
+                                  int32_t* d_iterations, int32_t use_graph, void* stream) {
+  if (!plan || !d_llr) return NRLDPC_ERR_ARG;
+  return execute(static_cast<MixedPlanImpl*>(plan), d_llr, d_bits, d_status, d_iterations, use_graph != 0,
+                 reinterpret_cast<cudaStream_t>(stream));
+}
+
+int32_t nrldpc_mixed_plan_autotune(void* plan, const int16_t* d_llr, uint8_t* d_bits, int32_t* d_status,
+                                   int32_t* d_iterations, float* ms_out, void* stream) {
+  if (!plan || !d_llr) return NRLDPC_ERR_ARG;
+  MixedPlanImpl* pl = static_cast<MixedPlanImpl*>(plan);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int cand[4][2] = {{2, 0}, {1, 0}, {2, 1}, {1, 1}};   // (CTAs per SM, work order)
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return NRLDPC_ERR_CUDA;
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int c = 0; c < 4; ++c) {
+    if (configure(pl, cand[c][0], cand[c][1]) != NRLDPC_OK) return NRLDPC_ERR_CUDA;
+    if (execute(pl, d_llr, d_bits, d_status, d_iterations, false, s) != NRLDPC_OK) return NRLDPC_ERR_CUDA;
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; ++r)
+      if (execute(pl, d_llr, d_bits, d_status, d_iterations, false, s) != NRLDPC_OK) return NRLDPC_ERR_CUDA;
+    cudaEventRecord(e1, s);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return NRLDPC_ERR_CUDA;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= 3.f;
+    if (ms_out) ms_out[c] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (configure(pl, cand[best][0], cand[best][1]) != NRLDPC_OK) return NRLDPC_ERR_CUDA;
+  return best;
+}
+
+int32_t nrldpc_mixed_plan_destroy(void* plan) {
+  if (plan) free_plan(static_cast<MixedPlanImpl*>(plan));
+  return NRLDPC_OK;
+}
+
+}  // extern "C"

@@ -234,6 +234,45 @@ int32_t nrldpc_channel_batch(const uint8_t *d_rm, int64_t rm_stride,
 /* Seed of tx_rx_process's noise generator (the reference uses srand()). */
 void nrldpc_channel_seed(uint64_t seed);
 
+/* ---- mixed-size batches (no counterpart in the reference) ---- */
+
+/* One code block of a mixed batch: its configuration (HARQ_on must be 0) and
+ * where its E LLRs (elements) and ceil(B/8) hard bits (bytes) live in the
+ * caller's LLR and output arenas. */
+typedef struct {
+    ldpc_in_config_t cfg;
+    int64_t llr_offset;
+    int64_t bits_offset;
+} nrldpc_block_t;
+
+/* Plan the decode of num_blocks blocks that may mix base graphs, lifting
+ * sizes, E, Qm, rv and CRC types, with one fixed-point decoder setting
+ * (algos 1-3).  Blocks of the same (BG, Zc) are paired into int16x2 lanes and
+ * grouped into work items that one persistent kernel pulls from a device work
+ * queue.  The plan owns its device tables and scratch.  Returns 0, -1, -2,
+ * -3 or -4. */
+int32_t nrldpc_mixed_plan_create(const nrldpc_block_t *blocks, int32_t num_blocks,
+                                 const ldpc_decoder_cfg_t *decoder_cfg, void **plan);
+
+/* Decode the planned batch: d_llr int16 arena, d_bits uint8 arena,
+ * d_status / d_iterations int32 [num_blocks] (nullable).  With use_graph != 0
+ * and a non-default stream, the launch (work-queue reset + kernel) is
+ * captured once into a CUDA graph and replayed; it is re-captured when the
+ * pointers, stream or tuning change.  Stream-ordered. */
+int32_t nrldpc_mixed_plan_execute(void *plan, const int16_t *d_llr, uint8_t *d_bits,
+                                  int32_t *d_status, int32_t *d_iterations,
+                                  int32_t use_graph, void *stream);
+
+/* Time the plan's candidate launch shapes (CTAs per SM 2 or 1) x work orders
+ * (largest items first / graphs interleaved) on the given data, keep the
+ * fastest and return its index (0..3); ms_out (nullable) receives the four
+ * mean times in ms.  Synchronises the stream. */
+int32_t nrldpc_mixed_plan_autotune(void *plan, const int16_t *d_llr, uint8_t *d_bits,
+                                   int32_t *d_status, int32_t *d_iterations,
+                                   float *ms_out, void *stream);
+
+int32_t nrldpc_mixed_plan_destroy(void *plan);
+
 /* Replace the per-(iteration, row) alpha/beta tables used by algo 2 for one
  * base graph (the reference compiles these in:
  * c_lib/BG1_trained_ldpc_weights.c:34,171, c_lib/BG2_trained_ldpc_weights.c).
