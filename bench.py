@@ -464,6 +464,117 @@ def run_mixed(args):
             "gpu_launches": int(launches)}
 
 
+TRAIN_CONFIGS = {"bg2_zc64": (2, 488, 1, 1920, 0, 2, 0), "bg1_zc112": (1, 2440, 1, 7392, 0, 2, 0)}
+
+
+def _train_cpu_baseline(cfg, T: int, batch: int = 64) -> dict:
+    """Forward + backward of the autograd restatement of the reference's unrolled
+    min-sum model on the host cores (the computation the reference trains with),
+    on a bounded batch."""
+    import torch
+
+    from oracle.minsum_torch import MinSumGraph, bce_loss, minsum_unrolled
+
+    torch.set_num_threads(os.cpu_count() or 1)
+    g = MinSumGraph(*cfg[:6])
+    gen = torch.Generator().manual_seed(0)
+    llr = (2.0 + 1.5 * torch.randn((batch, g.n), generator=gen))
+    target = torch.zeros((batch, g.B))
+    ra = torch.zeros((T, g.rows), requires_grad=True)
+    rb = torch.full((T, g.rows), -3.0, requires_grad=True)
+
+    def step():
+        a = 0.5 + 0.5 * torch.sigmoid(ra)
+        fin, _ = minsum_unrolled(g, llr, a, torch.sigmoid(rb))
+        bce_loss(fin, target, g.B).backward()
+
+    step()
+    t0 = time.perf_counter()
+    n = 0
+    while n < 3 or time.perf_counter() - t0 < 10.0:
+        step()
+        n += 1
+    dt = (time.perf_counter() - t0) / n
+    return {"value": round(batch / dt, 2), "unit": "codewords/s", "cores": torch.get_num_threads(), "kind": "port",
+            "sample": f"{n} forward+backward passes of batch {batch}, {T} iterations, torch autograd on host cores"}
+
+
+def run_train(args):
+    """Learned min-sum training step: device batch generation excluded, then
+    forward kernel + BCE loss + backward kernel + Adam step, per batch of 4096."""
+    import torch
+
+    from deeplearning_5g_ldpc_decoder_b200 import capi
+    from deeplearning_5g_ldpc_decoder_b200.train import (NeuralLayeredMinSumDecoder, decoder_loss,
+                                                         ebn0_to_noise_power_db, make_training_batch)
+
+    T = 10
+    batch = args.n_cw if args.n_cw != N_CW else 4096
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    base = None
+    if not args.no_cpu_baseline:
+        base = _train_cpu_baseline(TRAIN_CONFIGS["bg2_zc64"], T)
+    legs = {}
+    for name, cfg in TRAIN_CONFIGS.items():
+        model = NeuralLayeredMinSumDecoder(cfg, num_iterations=T, alpha_mode="checkpoint", init_alpha=0.7,
+                                           init_beta=0.02).to(dev)
+        opt = torch.optim.Adam(model.parameters(), lr=1e-2)
+        llr, target = make_training_batch(model, batch, ebn0_to_noise_power_db(1.5, cfg[5], model.B, cfg[3]), seed=3)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        fwd_ms = bwd_ms = 0.0
+
+        def step(timed):
+            nonlocal fwd_ms, bwd_ms
+            opt.zero_grad(set_to_none=True)
+            if timed:
+                ev[0].record()
+            _, final = model(llr, return_llr=True)
+            loss = decoder_loss(final, target, model.B)
+            if timed:
+                ev[1].record()
+            loss.backward()
+            if timed:
+                ev[2].record()
+            opt.step()
+            if timed:
+                ev[3].record()
+                torch.cuda.synchronize()
+                fwd_ms += ev[0].elapsed_time(ev[1])
+                bwd_ms += ev[1].elapsed_time(ev[2])
+
+        for _ in range(max(args.warmup, 3)):
+            step(False)
+        torch.cuda.synchronize()
+        l0 = capi.kernel_launch_count()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(args.steps):
+            step(False)
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / args.steps
+        launches = (capi.kernel_launch_count() - l0) // args.steps
+        for _ in range(3):
+            step(True)
+        n = model.n
+        ck_bytes = T * batch * (4 * n + 16 * model.num_rows * model.Zc)
+        legs[name] = {"ms_per_step": round(ms, 3), "codewords_per_s": round(batch / (ms * 1e-3), 1),
+                      "forward_ms": round(fwd_ms / 3, 3), "backward_ms": round(bwd_ms / 3, 3),
+                      "checkpoint_bytes": int(ck_bytes), "own_kernel_launches_per_step": int(launches),
+                      "n": n, "Zc": model.Zc, "B": model.B}
+    main = legs["bg2_zc64"]
+    return {"metric": "learned min-sum training throughput", "value": main["codewords_per_s"],
+            "unit": "codewords/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": main["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic: device-encoded random payloads, QPSK AWGN at Eb/N0 1.5 dB, int16 "
+                                    "LLRs rate-recovered on device",
+            "config": {"workload": f"learned min-sum training step, batch {batch}, {T} unrolled iterations, "
+                                   "checkpoint alpha/beta; BG2 Zc64 (A=488, E=1920) headline, BG1 Zc112 beside",
+                       "parallelism": "single GPU"},
+            "legs": legs, "cpu_baseline": base, "gpu_launches": main["own_kernel_launches_per_step"] * args.steps}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -474,8 +585,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n-cw", type=int, default=N_CW, help="code blocks per step (profiling runs use fewer)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
-    ap.add_argument("--workload", default="bg1_zc384", choices=["bg1_zc384", "mixed"],
-                    help="mixed: 32768 blocks over all 51 lifting sizes, BG1 60 %%, rate U[0.2, 0.92], Qm 2-8")
+    ap.add_argument("--workload", default="bg1_zc384", choices=["bg1_zc384", "mixed", "train"],
+                    help="mixed: 32768 blocks over all 51 lifting sizes, BG1 60 %%, rate U[0.2, 0.92], Qm 2-8; "
+                         "train: learned min-sum forward+backward, batch 4096, 10 iterations")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -502,6 +614,11 @@ def main():
         if rank != 0:
             return
         print(json.dumps(run_mixed(args)), flush=True)
+        return
+    if args.workload == "train":
+        if rank != 0:
+            return
+        print(json.dumps(run_train(args)), flush=True)
         return
 
     # The CPU baseline pool is spawned before any GPU work.

@@ -32,6 +32,7 @@ SOURCES = [
     "nrldpc_mixed.cu",
     "nrldpc_mixed_api.cu",
     "nrldpc_noalloc.cu",
+    "nrldpc_train.cu",
     "nrldpc_tables.cpp",
 ]
 HEADERS = [

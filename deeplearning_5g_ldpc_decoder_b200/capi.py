@@ -84,6 +84,8 @@ EXPORTED_SYMBOLS = (
     "nrldpc_decode_batch",
     "nrldpc_decode_batch_host",
     "nrldpc_decode_batch_noalloc",
+    "nrldpc_train_forward",
+    "nrldpc_train_backward",
     "nrldpc_set_trained_weights",
     "nrldpc_set_degree_alpha",
     "nrldpc_kernel_launch_count",
@@ -143,6 +145,12 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nrldpc_decode_batch_host.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig),
                                              ctypes.POINTER(DecoderConfig), vp, i64, vp, vp, vp]
     lib.nrldpc_decode_batch_host.restype = i32
+    f32 = ctypes.c_float
+    lib.nrldpc_train_forward.argtypes = [vp, i32, ctypes.POINTER(LdpcInConfig), i32, vp, vp, f32, vp, vp, vp, vp, vp]
+    lib.nrldpc_train_forward.restype = i32
+    lib.nrldpc_train_backward.argtypes = [vp, i32, ctypes.POINTER(LdpcInConfig), i32, vp, vp, f32, i32, vp, vp, vp,
+                                          vp, vp, vp, vp, vp]
+    lib.nrldpc_train_backward.restype = i32
     lib.nrldpc_set_trained_weights.argtypes = [ctypes.c_uint16, vp, vp, i32]
     lib.nrldpc_set_trained_weights.restype = i32
     lib.nrldpc_set_degree_alpha.argtypes = [vp]

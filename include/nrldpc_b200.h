@@ -273,6 +273,33 @@ int32_t nrldpc_mixed_plan_autotune(void *plan, const int16_t *d_llr, uint8_t *d_
 
 int32_t nrldpc_mixed_plan_destroy(void *plan);
 
+/* ---- differentiable unrolled float min-sum (no counterpart in the reference's
+ * C ABI; the training model it serves is deep_learning/deeplearning_ldpc_model.py) */
+
+/* Forward of `iterations` unrolled layered float min-sum iterations on batch
+ * decoder-layout LLRs d_llr float [batch][N+2Zc], with per-(iteration, row)
+ * d_alpha / d_beta float [iterations][rows], optional clip (<= 0: none).
+ * Writes d_final [batch][N+2Zc], optionally every iteration's LLRs d_iter
+ * [iterations][batch][N+2Zc], and the checkpoints the backward needs:
+ * d_ck_lq float [iterations][batch][N+2Zc] and d_ck_lr uint32
+ * [iterations][batch][rows][4][Zc].  No early termination. */
+int32_t nrldpc_train_forward(const float *d_llr, int32_t batch, const ldpc_in_config_t *cfg,
+                             int32_t iterations, const float *d_alpha, const float *d_beta,
+                             float clip, float *d_final, float *d_iter, float *d_ck_lq,
+                             uint32_t *d_ck_lr, void *stream);
+
+/* Backward of nrldpc_train_forward from its checkpoints: given the gradients
+ * of the final LLRs (d_g_final, nullable) and of every iteration's LLRs
+ * (d_g_iter, nullable), writes d_g_llr [batch][N+2Zc] and ADDS into d_g_alpha /
+ * d_g_beta [iterations][rows].  detach != 0 stops gradients through the check
+ * update inputs (the model's detach_check_update_inputs). */
+int32_t nrldpc_train_backward(const float *d_llr, int32_t batch, const ldpc_in_config_t *cfg,
+                              int32_t iterations, const float *d_alpha, const float *d_beta,
+                              float clip, int32_t detach, const float *d_ck_lq,
+                              const uint32_t *d_ck_lr, const float *d_g_final,
+                              const float *d_g_iter, float *d_g_llr, float *d_g_alpha,
+                              float *d_g_beta, void *stream);
+
 /* Replace the per-(iteration, row) alpha/beta tables used by algo 2 for one
  * base graph (the reference compiles these in:
  * c_lib/BG1_trained_ldpc_weights.c:34,171, c_lib/BG2_trained_ldpc_weights.c).

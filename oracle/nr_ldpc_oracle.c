@@ -66,6 +66,17 @@ static const graph_t *graph(int bgn) {
     return &g_graph[bgn == 1 ? 0 : 1];
 }
 
+int orc_graph(const orc_params_t *p, int32_t *col, int32_t *shift, int32_t *off) {
+    if (!p || (p->bgn != 1 && p->bgn != 2) || p->Zc <= 0) return -1;
+    const graph_t *g = graph(p->bgn);
+    for (int i = 0; i < g->nnz; i++) {
+        col[i] = g->col[i];
+        shift[i] = g->v[p->iLS][i] % p->Zc;
+    }
+    for (int r = 0; r <= g->rows; r++) off[r] = g->off[r];
+    return g->nnz;
+}
+
 /* ------------------------------------------------------------ parameters */
 /* c_lib/ldpc_internal.c:13-22 (TS 38.212 Table 5.3.2-1) and :24-64. */
 static const int kSets[8][8] = {

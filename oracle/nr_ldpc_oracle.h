@@ -39,6 +39,12 @@ typedef struct {
 /* gen_ldpc_parameters (c_lib/ldpc_internal.c:66-170). 0 ok, -1 invalid. */
 int orc_derive(const orc_in_config_t *in, orc_params_t *p);
 
+/* Base-graph tables of one configuration in the reference's CSR layout
+ * (ldpc_config_t of c_lib/nr_ldpc.h: HBG_array / Vij_array / HBG_offset_array):
+ * col[nnz] base columns, shift[nnz] = Vij mod Zc for the configuration's
+ * lifting set, off[rows+1] row offsets.  Returns nnz, or -1. */
+int orc_graph(const orc_params_t *p, int32_t *col, int32_t *shift, int32_t *off);
+
 /* calculate_crc (c_lib/nr_crc.c:170-179). */
 uint32_t orc_crc(const uint8_t *data, int len, int crctype);
 

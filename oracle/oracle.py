@@ -100,12 +100,25 @@ class Oracle:
         L.orc_channel.restype = ctypes.c_int
         L.orc_set_trained.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.orc_set_degree_alpha.argtypes = [ctypes.c_void_p]
+        L.orc_graph.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_graph.restype = ctypes.c_int
         self.harq = np.zeros(68 * 384, dtype=np.int16)
 
     def derive(self, cfg: InConfig):
         p = OrcParams()
         rc = self.lib.orc_derive(ctypes.byref(cfg), ctypes.byref(p))
         return rc, p
+
+    def graph(self, cfg: InConfig):
+        """(params, col[nnz], shift[nnz] = Vij mod Zc, off[rows+1]) of one configuration."""
+        rc, p = self.derive(cfg)
+        if rc != 0:
+            raise ValueError("invalid LDPC configuration")
+        col = np.zeros(316, dtype=np.int32)
+        shift = np.zeros(316, dtype=np.int32)
+        off = np.zeros(47, dtype=np.int32)
+        nnz = self.lib.orc_graph(ctypes.byref(p), _p(col), _p(shift), _p(off))
+        return p, col[:nnz].copy(), shift[:nnz].copy(), off[: p.rows + 1].copy()
 
     def crc(self, data: np.ndarray, crctype: int) -> int:
         data = np.ascontiguousarray(data, dtype=np.uint8)
