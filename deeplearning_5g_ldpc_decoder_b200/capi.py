@@ -86,6 +86,9 @@ EXPORTED_SYMBOLS = (
     "nrldpc_decode_batch_noalloc",
     "nrldpc_train_forward",
     "nrldpc_train_backward",
+    "nrldpc_train_forward_f64",
+    "nrldpc_train_backward_f64",
+    "nrldpc_train_checkpoint_words",
     "nrldpc_set_trained_weights",
     "nrldpc_set_degree_alpha",
     "nrldpc_kernel_launch_count",
@@ -151,6 +154,16 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nrldpc_train_backward.argtypes = [vp, i32, ctypes.POINTER(LdpcInConfig), i32, vp, vp, f32, i32, vp, vp, vp,
                                           vp, vp, vp, vp, vp]
     lib.nrldpc_train_backward.restype = i32
+    f64 = ctypes.c_double
+    lib.nrldpc_train_forward_f64.argtypes = [vp, i32, ctypes.POINTER(LdpcInConfig), i32, vp, vp, f64, vp, vp, vp, vp,
+                                             vp]
+    lib.nrldpc_train_forward_f64.restype = i32
+    lib.nrldpc_train_backward_f64.argtypes = [vp, i32, ctypes.POINTER(LdpcInConfig), i32, vp, vp, f64, i32, vp, vp,
+                                              vp, vp, vp, vp, vp, vp]
+    lib.nrldpc_train_backward_f64.restype = i32
+    lib.nrldpc_train_checkpoint_words.argtypes = [ctypes.POINTER(LdpcInConfig), i32, i32, i32,
+                                                  ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    lib.nrldpc_train_checkpoint_words.restype = i32
     lib.nrldpc_set_trained_weights.argtypes = [ctypes.c_uint16, vp, vp, i32]
     lib.nrldpc_set_trained_weights.restype = i32
     lib.nrldpc_set_degree_alpha.argtypes = [vp]

@@ -452,29 +452,99 @@ int32_t encode_one(uint8_t* infobytes, uint8_t* rm_bytes, ldpc_in_config_t* inco
   return NRLDPC_OK;
 }
 
-// Launch geometry of the training kernels for one configuration.
-int make_train_params(const ldpc_in_config_t* cfg, int32_t T, int32_t batch, float clip, TrainParams* p, int* block,
-                      int* smem_fwd, int* smem_bwd) {
+// Launch geometry of the training kernels for one configuration.  The float64
+// variant needs 2 (N+2Zc) doubles of shared memory per code block in the
+// backward, so it runs fewer blocks per CTA (and not at all where one does not fit).
+int make_train_params(const ldpc_in_config_t* cfg, int32_t T, int32_t batch, double clip, bool f64, TrainParams* p,
+                      int* block, int* smem_fwd, int* smem_bwd) {
   CodeParams cp;
   if (!cfg || derive_params(*cfg, &cp, true) != 0) return NRLDPC_ERR_CONFIG;
   if (T < 1 || batch < 0) return NRLDPC_ERR_ARG;
   memset(p, 0, sizeof(*p));
   const BaseGraph& g = base_graph(cp.bgn);
+  const int real = f64 ? 8 : 4;
+  const int smem_cap = 227 * 1024 - 1024;   // opt-in shared memory per block, less the static reduction buffer
+  int G = std::max(1, kThreadsTarget / cp.Zc);
+  while (G > 1 && 2 * G * cp.lq_len * real > smem_cap) --G;
+  if (2 * G * cp.lq_len * real > smem_cap) return NRLDPC_ERR_CONFIG;
   p->Zc = cp.Zc;
   p->R = g.rows;
   p->n = cp.lq_len;
-  p->G = std::max(1, kThreadsTarget / cp.Zc);
+  p->G = G;
   p->nnz = g.nnz;
   p->T = T;
   p->batch = batch;
-  p->clip = clip > 0.0f ? clip : INFINITY;
+  p->msg_words = (f64 ? 6 : 4) * cp.Zc;
+  p->clip = clip > 0.0 ? clip : INFINITY;
   for (int e = 0; e < g.nnz; ++e)
     p->edge[e] = (uint32_t)g.col[e] * (uint32_t)cp.Zc | ((uint32_t)(g.vij[cp.iLS][e] % cp.Zc) << 16);
   for (int r = 0; r <= g.rows; ++r) p->row_off[r] = g.row_off[r];
   *block = (p->G * cp.Zc + 31) & ~31;
-  *smem_fwd = p->G * cp.lq_len * 4;
-  *smem_bwd = 2 * p->G * cp.lq_len * 4;
+  *smem_fwd = p->G * cp.lq_len * real;
+  *smem_bwd = 2 * p->G * cp.lq_len * real;
   return NRLDPC_OK;
+}
+
+int train_forward(const void* d_llr, int32_t batch, const ldpc_in_config_t* cfg, int32_t iterations,
+                  const void* d_alpha, const void* d_beta, double clip, void* d_final, void* d_iter, void* d_ck_lq,
+                  uint32_t* d_ck_lr, void* stream, bool f64) {
+  TrainParams p;
+  int block, smem_f, smem_b;
+  const int rc = make_train_params(cfg, iterations, batch, clip, f64, &p, &block, &smem_f, &smem_b);
+  if (rc != NRLDPC_OK) return rc;
+  if (batch == 0) return NRLDPC_OK;
+  if (!d_llr || !d_alpha || !d_beta || !d_final || !d_ck_lq || !d_ck_lr) return NRLDPC_ERR_ARG;
+  p.llr = d_llr;
+  p.alpha = d_alpha;
+  p.beta = d_beta;
+  p.final_llr = d_final;
+  p.iter_llr = d_iter;
+  p.ck_lq = d_ck_lq;
+  p.ck_lr = d_ck_lr;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int occ = std::max(1, occupancy_train(false, f64, block, smem_f));
+  const int items = (batch + p.G - 1) / p.G;
+  const int grid = std::max(1, std::min(items, occ * sms));
+  return launch_train_forward(p, f64, grid, block, smem_f, stream) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
+}
+
+int train_backward(const void* d_llr, int32_t batch, const ldpc_in_config_t* cfg, int32_t iterations,
+                   const void* d_alpha, const void* d_beta, double clip, int32_t detach, const void* d_ck_lq,
+                   const uint32_t* d_ck_lr, const void* d_g_final, const void* d_g_iter, void* d_g_llr,
+                   void* d_g_alpha, void* d_g_beta, void* stream, bool f64) {
+  TrainParams p;
+  int block, smem_f, smem_b;
+  const int rc = make_train_params(cfg, iterations, batch, clip, f64, &p, &block, &smem_f, &smem_b);
+  if (rc != NRLDPC_OK) return rc;
+  if (batch == 0) return NRLDPC_OK;
+  if (!d_llr || !d_alpha || !d_beta || !d_ck_lq || !d_ck_lr || !d_g_llr || !d_g_alpha || !d_g_beta)
+    return NRLDPC_ERR_ARG;
+  p.llr = d_llr;
+  p.alpha = d_alpha;
+  p.beta = d_beta;
+  p.detach = detach ? 1 : 0;
+  p.ck_lq = const_cast<void*>(d_ck_lq);
+  p.ck_lr = const_cast<uint32_t*>(d_ck_lr);
+  p.g_final = d_g_final;
+  p.g_iter = d_g_iter;
+  p.g_llr = d_g_llr;
+  p.g_alpha = d_g_alpha;
+  p.g_beta = d_g_beta;
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
+  const int occ = std::max(1, occupancy_train(true, f64, block, smem_b));
+  const int items = (batch + p.G - 1) / p.G;
+  const int grid = std::max(1, std::min(items, occ * st->num_sms));
+  p.scratch_per_cta = (int64_t)p.G * p.nnz * p.Zc;
+  const size_t real = f64 ? 8 : 4;
+  Buffer& b = st->train_scratch[reinterpret_cast<cudaStream_t>(stream)];
+  if (ensure(&b, 2 * real * (size_t)grid * (size_t)p.scratch_per_cta)) return NRLDPC_ERR_CUDA;
+  p.tape = b.ptr;
+  p.carry = static_cast<char*>(b.ptr) + real * (size_t)grid * (size_t)p.scratch_per_cta;
+  return launch_train_backward(p, f64, grid, block, smem_b, stream) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
 }
 
 }  // namespace
@@ -706,26 +776,8 @@ int tx_rx_process(const uint8_t* inbytes, size_t num_bits, uint16_t Qm, float no
 int32_t nrldpc_train_forward(const float* d_llr, int32_t batch, const ldpc_in_config_t* cfg, int32_t iterations,
                              const float* d_alpha, const float* d_beta, float clip, float* d_final, float* d_iter,
                              float* d_ck_lq, uint32_t* d_ck_lr, void* stream) {
-  TrainParams p;
-  int block, smem_f, smem_b;
-  const int rc = make_train_params(cfg, iterations, batch, clip, &p, &block, &smem_f, &smem_b);
-  if (rc != NRLDPC_OK) return rc;
-  if (batch == 0) return NRLDPC_OK;
-  if (!d_llr || !d_alpha || !d_beta || !d_final || !d_ck_lq || !d_ck_lr) return NRLDPC_ERR_ARG;
-  p.llr = d_llr;
-  p.alpha = d_alpha;
-  p.beta = d_beta;
-  p.final_llr = d_final;
-  p.iter_llr = d_iter;
-  p.ck_lq = d_ck_lq;
-  p.ck_lr = d_ck_lr;
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int occ = std::max(1, occupancy_train(false, block, smem_f));
-  const int items = (batch + p.G - 1) / p.G;
-  const int grid = std::max(1, std::min(items, occ * sms));
-  return launch_train_forward(p, grid, block, smem_f, stream) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
+  return train_forward(d_llr, batch, cfg, iterations, d_alpha, d_beta, clip, d_final, d_iter, d_ck_lq, d_ck_lr, stream,
+                       false);
 }
 
 int32_t nrldpc_train_backward(const float* d_llr, int32_t batch, const ldpc_in_config_t* cfg, int32_t iterations,
@@ -733,36 +785,35 @@ int32_t nrldpc_train_backward(const float* d_llr, int32_t batch, const ldpc_in_c
                               const float* d_ck_lq, const uint32_t* d_ck_lr, const float* d_g_final,
                               const float* d_g_iter, float* d_g_llr, float* d_g_alpha, float* d_g_beta,
                               void* stream) {
+  return train_backward(d_llr, batch, cfg, iterations, d_alpha, d_beta, clip, detach, d_ck_lq, d_ck_lr, d_g_final,
+                        d_g_iter, d_g_llr, d_g_alpha, d_g_beta, stream, false);
+}
+
+int32_t nrldpc_train_forward_f64(const double* d_llr, int32_t batch, const ldpc_in_config_t* cfg,
+                                 int32_t iterations, const double* d_alpha, const double* d_beta, double clip,
+                                 double* d_final, double* d_iter, double* d_ck_lq, uint32_t* d_ck_lr, void* stream) {
+  return train_forward(d_llr, batch, cfg, iterations, d_alpha, d_beta, clip, d_final, d_iter, d_ck_lq, d_ck_lr, stream,
+                       true);
+}
+
+int32_t nrldpc_train_backward_f64(const double* d_llr, int32_t batch, const ldpc_in_config_t* cfg,
+                                  int32_t iterations, const double* d_alpha, const double* d_beta, double clip,
+                                  int32_t detach, const double* d_ck_lq, const uint32_t* d_ck_lr,
+                                  const double* d_g_final, const double* d_g_iter, double* d_g_llr,
+                                  double* d_g_alpha, double* d_g_beta, void* stream) {
+  return train_backward(d_llr, batch, cfg, iterations, d_alpha, d_beta, clip, detach, d_ck_lq, d_ck_lr, d_g_final,
+                        d_g_iter, d_g_llr, d_g_alpha, d_g_beta, stream, true);
+}
+
+int32_t nrldpc_train_checkpoint_words(const ldpc_in_config_t* cfg, int32_t iterations, int32_t batch,
+                                      int32_t f64, int64_t* lq_elems, int64_t* msg_words) {
   TrainParams p;
   int block, smem_f, smem_b;
-  const int rc = make_train_params(cfg, iterations, batch, clip, &p, &block, &smem_f, &smem_b);
+  const int rc = make_train_params(cfg, iterations, batch, 0.0, f64 != 0, &p, &block, &smem_f, &smem_b);
   if (rc != NRLDPC_OK) return rc;
-  if (batch == 0) return NRLDPC_OK;
-  if (!d_llr || !d_alpha || !d_beta || !d_ck_lq || !d_ck_lr || !d_g_llr || !d_g_alpha || !d_g_beta)
-    return NRLDPC_ERR_ARG;
-  p.llr = d_llr;
-  p.alpha = d_alpha;
-  p.beta = d_beta;
-  p.detach = detach ? 1 : 0;
-  p.ck_lq = const_cast<float*>(d_ck_lq);
-  p.ck_lr = const_cast<uint32_t*>(d_ck_lr);
-  p.g_final = d_g_final;
-  p.g_iter = d_g_iter;
-  p.g_llr = d_g_llr;
-  p.g_alpha = d_g_alpha;
-  p.g_beta = d_g_beta;
-  std::lock_guard<std::mutex> lock(g_mu);
-  DeviceState* st = nullptr;
-  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
-  const int occ = std::max(1, occupancy_train(true, block, smem_b));
-  const int items = (batch + p.G - 1) / p.G;
-  const int grid = std::max(1, std::min(items, occ * st->num_sms));
-  p.scratch_per_cta = (int64_t)p.G * p.nnz * p.Zc;
-  Buffer& b = st->train_scratch[reinterpret_cast<cudaStream_t>(stream)];
-  if (ensure(&b, 2 * sizeof(float) * (size_t)grid * (size_t)p.scratch_per_cta)) return NRLDPC_ERR_CUDA;
-  p.tape = static_cast<float*>(b.ptr);
-  p.carry = p.tape + (size_t)grid * p.scratch_per_cta;
-  return launch_train_backward(p, grid, block, smem_b, stream) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
+  if (lq_elems) *lq_elems = (int64_t)iterations * batch * p.n;
+  if (msg_words) *msg_words = (int64_t)iterations * batch * p.R * p.msg_words;
+  return NRLDPC_OK;
 }
 
 }  // extern "C"

@@ -152,31 +152,33 @@ struct MixedParams {
 // ---- differentiable unrolled float min-sum (training) ----
 struct TrainParams {
   int32_t Zc, R, n, G, nnz, T, batch, detach;
-  float clip;                 // +inf when LLRs are not clipped
-  const float* llr;           // [batch][n] decoder-layout input LLRs
-  const float* alpha;         // [T][R]
-  const float* beta;          // [T][R]
-  float* final_llr;           // [batch][n]
-  float* iter_llr;            // [T][batch][n] or null
-  float* ck_lq;               // [T][batch][n] LQ at the start of each iteration
-  uint32_t* ck_lr;            // [T][batch][R][4][Zc] compressed messages at the start of each iteration
-  const float* g_final;       // [batch][n] or null
-  const float* g_iter;        // [T][batch][n] or null
-  float* g_llr;               // [batch][n]
-  float* g_alpha;             // [T][R], accumulated
-  float* g_beta;              // [T][R], accumulated
-  float* tape;                // per CTA: G * nnz * Zc
-  float* carry;               // per CTA: G * nnz * Zc
-  int64_t scratch_per_cta;    // floats of tape (and of carry) per CTA
+  int32_t msg_words;          // 32-bit words of compressed messages per lifted row block (4 Zc f32, 6 Zc f64)
+  double clip;                // +inf when LLRs are not clipped
+  // Real = float or double, per the entry point.
+  const void* llr;            // Real [batch][n] decoder-layout input LLRs
+  const void* alpha;          // Real [T][R]
+  const void* beta;           // Real [T][R]
+  void* final_llr;            // Real [batch][n]
+  void* iter_llr;             // Real [T][batch][n] or null
+  void* ck_lq;                // Real [T][batch][n] LQ at the start of each iteration
+  uint32_t* ck_lr;            // [T][batch][R][msg_words]: Real m1[Zc], m2[Zc]; u32 flips[Zc], first-min index[Zc]
+  const void* g_final;        // Real [batch][n] or null
+  const void* g_iter;         // Real [T][batch][n] or null
+  void* g_llr;                // Real [batch][n]
+  void* g_alpha;              // Real [T][R], accumulated
+  void* g_beta;               // Real [T][R], accumulated
+  void* tape;                 // per CTA: G * nnz * Zc Real
+  void* carry;                // per CTA: G * nnz * Zc Real
+  int64_t scratch_per_cta;    // elements of tape (and of carry) per CTA
   uint32_t edge[kMaxNnz];     // base column * Zc in the low 16 bits, V mod Zc in the high
   uint16_t row_off[kMaxRows + 1];
 };
 
 // Kernel launchers (defined in the .cu files).  Return a cudaError_t value.
 int launch_encode(const EncodeParams& p, void* stream);
-int launch_train_forward(const TrainParams& p, int grid, int block, int smem, void* stream);
-int launch_train_backward(const TrainParams& p, int grid, int block, int smem, void* stream);
-int occupancy_train(bool backward, int block, int smem);
+int launch_train_forward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream);
+int launch_train_backward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream);
+int occupancy_train(bool backward, bool f64, int block, int smem);
 int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream);
 int prepare_mixed(bool degen_clip);
 int occupancy_mixed(bool degen_clip);

@@ -25,6 +25,10 @@
 // to the returned index, abs to sign(x), clamp to its pass-through mask).
 // Memory: O(iterations x state) for checkpoints, O(state) for tape and carry,
 // instead of every intermediate tensor autograd would keep.
+//
+// Both kernels are templates over the real type: float is the training type;
+// double exists so gradients can be checked against central finite differences
+// without float32 rounding noise (the role float64 plays in torch's gradcheck).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -34,6 +38,17 @@
 namespace nrldpc {
 namespace {
 
+// Correctly rounded arithmetic in the kernel's real type (no FMA contraction,
+// matching torch's separate elementwise ops).
+__device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float r_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double r_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double r_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a, b); }
+template <typename Real>
+__device__ __forceinline__ Real r_inf() { return (Real)INFINITY; }
+
 __device__ __forceinline__ uint32_t tr_addr(const TrainParams& p, int e, uint32_t zx) {
   const uint32_t ed = p.edge[e];
   uint32_t t = zx + (ed >> 16);
@@ -41,37 +56,51 @@ __device__ __forceinline__ uint32_t tr_addr(const TrainParams& p, int e, uint32_
   return (ed & 0xFFFFu) + t;
 }
 
+// Compressed messages of one lifted row block: Real m1[Zc], m2[Zc], then
+// uint32 flips[Zc], first-minimum index[Zc].
+template <typename Real>
+struct MsgBlock {
+  Real* mag;
+  uint32_t* bits;
+  __device__ MsgBlock(uint32_t* base, int row, int msg_words, int Zc) {
+    uint32_t* b = base + (size_t)row * msg_words;
+    mag = reinterpret_cast<Real*>(b);
+    bits = b + 2 * Zc * (int)(sizeof(Real) / 4);
+  }
+};
+
 // Forward of one lifted check row.  Old messages come from the checkpoint of
 // iteration t (zero at t == 0); new messages go to the checkpoint of t+1.
-template <int D>
-__device__ __forceinline__ void train_row_fwd(const TrainParams& p, float* __restrict__ lq, uint32_t zx, int e0,
-                                              int row, float alpha, float beta, const uint32_t* old_msg,
-                                              uint32_t* new_msg, float* tape) {
+template <int D, typename Real>
+__device__ __forceinline__ void train_row_fwd(const TrainParams& p, Real* __restrict__ lq, uint32_t zx, int e0,
+                                              int row, Real alpha, Real beta, uint32_t* old_msg,
+                                              uint32_t* new_msg, Real* tape) {
   const int Zc = p.Zc;
-  float n1 = 0.f, n2 = 0.f;
+  const Real clip = (Real)p.clip;
+  Real n1 = 0, n2 = 0;
   uint32_t fl = 0u, ix = 0u;
   if (old_msg) {
-    const uint32_t* m = old_msg + (size_t)row * 4 * Zc + zx;
-    n1 = __uint_as_float(m[0]);
-    n2 = __uint_as_float(m[Zc]);
-    fl = m[2 * Zc];
-    ix = m[3 * Zc];
+    MsgBlock<Real> m(old_msg, row, p.msg_words, Zc);
+    n1 = m.mag[zx];
+    n2 = m.mag[Zc + zx];
+    fl = m.bits[zx];
+    ix = m.bits[Zc + zx];
   }
-  float rel[D];
+  Real rel[D];
   uint32_t addr[D];
   bool neg = false;
-  float m1 = INFINITY, m2 = INFINITY;
+  Real m1 = r_inf<Real>(), m2 = r_inf<Real>();
   int idx = 0;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
     addr[j] = tr_addr(p, e0 + j, zx);
-    float old = ((int)ix == j) ? n2 : n1;
+    Real old = ((int)ix == j) ? n2 : n1;
     old = ((fl >> j) & 1u) ? -old : old;
-    const float r = __fsub_rn(lq[addr[j]], old);
+    const Real r = r_sub(lq[addr[j]], old);
     rel[j] = r;
     if (tape) tape[(size_t)(e0 + j) * Zc + zx] = r;
-    neg ^= (r < 0.0f);
-    const float a = fabsf(r);
+    neg ^= (r < (Real)0);
+    const Real a = fabs(r);
     if (a < m1) {
       m2 = m1;
       m1 = a;
@@ -80,45 +109,45 @@ __device__ __forceinline__ void train_row_fwd(const TrainParams& p, float* __res
       m2 = a;
     }
   }
-  const float s1 = __fmul_rn(alpha, fmaxf(__fsub_rn(m1, beta), 0.0f));
-  const float s2 = __fmul_rn(alpha, fmaxf(__fsub_rn(m2, beta), 0.0f));
+  const Real s1 = r_mul(alpha, fmax(r_sub(m1, beta), (Real)0));
+  const Real s2 = r_mul(alpha, fmax(r_sub(m2, beta), (Real)0));
   uint32_t flips = 0u;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    const bool flip = (rel[j] < 0.0f) != neg;
-    const float mag = (j == idx) ? s2 : s1;
-    const float lr = flip ? -mag : mag;
+    const bool flip = (rel[j] < (Real)0) != neg;
+    const Real mag = (j == idx) ? s2 : s1;
     flips |= (flip ? 1u : 0u) << j;
-    float v = __fadd_rn(rel[j], lr);
-    v = fminf(fmaxf(v, -p.clip), p.clip);
+    Real v = r_add(rel[j], flip ? -mag : mag);
+    v = fmin(fmax(v, -clip), clip);
     lq[addr[j]] = v;
   }
   if (new_msg) {
-    uint32_t* m = new_msg + (size_t)row * 4 * Zc + zx;
-    m[0] = __float_as_uint(s1);
-    m[Zc] = __float_as_uint(s2);
-    m[2 * Zc] = flips;
-    m[3 * Zc] = (uint32_t)idx;
+    MsgBlock<Real> m(new_msg, row, p.msg_words, Zc);
+    m.mag[zx] = s1;
+    m.mag[Zc + zx] = s2;
+    m.bits[zx] = flips;
+    m.bits[Zc + zx] = (uint32_t)idx;
   }
 }
 
 // Backward of one lifted check row (see the file comment).
-template <int D>
-__device__ __forceinline__ void train_row_bwd(const TrainParams& p, float* __restrict__ glq, uint32_t zx, int e0,
-                                              float alpha, float beta, const float* tape, float* carry, float* ga,
-                                              float* gb) {
+template <int D, typename Real>
+__device__ __forceinline__ void train_row_bwd(const TrainParams& p, Real* __restrict__ glq, uint32_t zx, int e0,
+                                              Real alpha, Real beta, const Real* tape, Real* carry, Real* ga,
+                                              Real* gb) {
   const int Zc = p.Zc;
-  float rel[D];
+  const Real clip = (Real)p.clip;
+  Real rel[D];
   uint32_t addr[D];
   bool neg = false;
-  float m1 = INFINITY, m2 = INFINITY;
+  Real m1 = r_inf<Real>(), m2 = r_inf<Real>();
   int idx = 0, idx2 = -1;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
     addr[j] = tr_addr(p, e0 + j, zx);
     rel[j] = tape[(size_t)(e0 + j) * Zc + zx];
-    neg ^= (rel[j] < 0.0f);
-    const float a = fabsf(rel[j]);
+    neg ^= (rel[j] < (Real)0);
+    const Real a = fabs(rel[j]);
     if (a < m1) {
       m2 = m1;
       m1 = a;
@@ -129,35 +158,35 @@ __device__ __forceinline__ void train_row_bwd(const TrainParams& p, float* __res
   }
   // idx2 as torch.min over the entries other than idx: first strict minimum.
   {
-    float best = INFINITY;
+    Real best = r_inf<Real>();
 #pragma unroll
     for (int j = 0; j < D; ++j) {
-      const float a = fabsf(rel[j]);
+      const Real a = fabs(rel[j]);
       if (j != idx && a < best) {
         best = a;
         idx2 = j;
       }
     }
   }
-  const float o1 = __fsub_rn(m1, beta), o2 = __fsub_rn(m2, beta);
-  const float r1 = fmaxf(o1, 0.0f), r2 = fmaxf(o2, 0.0f);
-  const float k1 = o1 >= 0.0f ? alpha : 0.0f;   // d mag / d u
-  const float k2 = o2 >= 0.0f ? alpha : 0.0f;
-  const float s1 = __fmul_rn(alpha, r1), s2 = __fmul_rn(alpha, r2);
-  float g_a_idx = 0.0f, g_a_idx2 = 0.0f;
-  float g_new[D], g_mag_sum_r = 0.0f, g_u_sum = 0.0f;
+  const Real o1 = r_sub(m1, beta), o2 = r_sub(m2, beta);
+  const Real r1 = fmax(o1, (Real)0), r2 = fmax(o2, (Real)0);
+  const Real k1 = o1 >= (Real)0 ? alpha : (Real)0;   // d mag / d u
+  const Real k2 = o2 >= (Real)0 ? alpha : (Real)0;
+  const Real s1 = r_mul(alpha, r1), s2 = r_mul(alpha, r2);
+  Real g_a_idx = 0, g_a_idx2 = 0;
+  Real g_new[D], g_mag_sum_r = 0, g_u_sum = 0;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    const bool flip = (rel[j] < 0.0f) != neg;
-    const float mag = (j == idx) ? s2 : s1;
-    const float v = __fadd_rn(rel[j], flip ? -mag : mag);
-    const float gv = (v >= -p.clip && v <= p.clip) ? glq[addr[j]] : 0.0f;
+    const bool flip = (rel[j] < (Real)0) != neg;
+    const Real mag = (j == idx) ? s2 : s1;
+    const Real v = r_add(rel[j], flip ? -mag : mag);
+    const Real gv = (v >= -clip && v <= clip) ? glq[addr[j]] : (Real)0;
     g_new[j] = gv;
-    float* cr = carry + (size_t)(e0 + j) * Zc + zx;
-    const float g_lrt = *cr + gv;
-    const float g_mag = flip ? -g_lrt : g_lrt;
+    Real* cr = carry + (size_t)(e0 + j) * Zc + zx;
+    const Real g_lrt = *cr + gv;
+    const Real g_mag = flip ? -g_lrt : g_lrt;
     g_mag_sum_r += g_mag * ((j == idx) ? r2 : r1);
-    const float g_u = g_mag * ((j == idx) ? k2 : k1);
+    const Real g_u = g_mag * ((j == idx) ? k2 : k1);
     g_u_sum += g_u;
     if (j == idx) {
       g_a_idx2 += g_u;
@@ -169,12 +198,12 @@ __device__ __forceinline__ void train_row_bwd(const TrainParams& p, float* __res
   *gb -= g_u_sum;
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    float g_rel = 0.0f;
+    Real g_rel = 0;
     if (!p.detach) {
-      float g_a = 0.0f;
+      Real g_a = 0;
       if (j == idx) g_a += g_a_idx;
       if (j == idx2) g_a += g_a_idx2;
-      const float sg = rel[j] > 0.0f ? 1.0f : (rel[j] < 0.0f ? -1.0f : 0.0f);
+      const Real sg = rel[j] > (Real)0 ? (Real)1 : (rel[j] < (Real)0 ? (Real)-1 : (Real)0);
       g_rel = g_new[j] + g_a * sg;
     }
     glq[addr[j]] = g_rel;
@@ -182,102 +211,124 @@ __device__ __forceinline__ void train_row_bwd(const TrainParams& p, float* __res
   }
 }
 
-#define NRLDPC_TRAIN_DISPATCH(FN, deg, ...)   \
-  switch (deg) {                              \
-    case 3: FN<3>(__VA_ARGS__); break;        \
-    case 4: FN<4>(__VA_ARGS__); break;        \
-    case 5: FN<5>(__VA_ARGS__); break;        \
-    case 6: FN<6>(__VA_ARGS__); break;        \
-    case 7: FN<7>(__VA_ARGS__); break;        \
-    case 8: FN<8>(__VA_ARGS__); break;        \
-    case 9: FN<9>(__VA_ARGS__); break;        \
-    case 10: FN<10>(__VA_ARGS__); break;      \
-    default: FN<19>(__VA_ARGS__); break;      \
+#define NRLDPC_TRAIN_DISPATCH(FN, R, deg, ...)   \
+  switch (deg) {                                 \
+    case 3: FN<3, R>(__VA_ARGS__); break;        \
+    case 4: FN<4, R>(__VA_ARGS__); break;        \
+    case 5: FN<5, R>(__VA_ARGS__); break;        \
+    case 6: FN<6, R>(__VA_ARGS__); break;        \
+    case 7: FN<7, R>(__VA_ARGS__); break;        \
+    case 8: FN<8, R>(__VA_ARGS__); break;        \
+    case 9: FN<9, R>(__VA_ARGS__); break;        \
+    case 10: FN<10, R>(__VA_ARGS__); break;      \
+    default: FN<19, R>(__VA_ARGS__); break;      \
   }
 
+template <typename Real>
 __global__ void __launch_bounds__(kThreadsTarget) train_forward_kernel(const __grid_constant__ TrainParams p) {
-  extern __shared__ __align__(16) float s_lqf[];
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  Real* s_lq = reinterpret_cast<Real*>(s_raw);
+  const Real* llr = static_cast<const Real*>(p.llr);
+  const Real* alpha_t = static_cast<const Real*>(p.alpha);
+  const Real* beta_t = static_cast<const Real*>(p.beta);
+  Real* final_llr = static_cast<Real*>(p.final_llr);
+  Real* iter_llr = static_cast<Real*>(p.iter_llr);
+  Real* ck_lq = static_cast<Real*>(p.ck_lq);
+  const Real clip = (Real)p.clip;
   const int tid = threadIdx.x;
   const int g = tid / p.Zc, zx = tid - g * p.Zc;
   const bool active = g < p.G;
-  float* lq = s_lqf + (active ? g : 0) * p.n;
-  const size_t msg_words = (size_t)p.R * 4 * p.Zc;
+  Real* lq = s_lq + (active ? g : 0) * p.n;
+  const size_t cw_words = (size_t)p.R * p.msg_words;
   for (int item = blockIdx.x; item * p.G < p.batch; item += gridDim.x) {
     const int cw = item * p.G + g;
     const bool valid = active && cw < p.batch;
     if (valid)
-      for (int i = zx; i < p.n; i += p.Zc) lq[i] = fminf(fmaxf(p.llr[(size_t)cw * p.n + i], -p.clip), p.clip);
+      for (int i = zx; i < p.n; i += p.Zc) lq[i] = fmin(fmax(llr[(size_t)cw * p.n + i], -clip), clip);
     __syncthreads();
     for (int t = 0; t < p.T; ++t) {
       if (valid)
-        for (int i = zx; i < p.n; i += p.Zc) p.ck_lq[((size_t)t * p.batch + cw) * p.n + i] = lq[i];
-      const uint32_t* old_msg = (t > 0 && valid) ? p.ck_lr + ((size_t)t * p.batch + cw) * msg_words : nullptr;
-      uint32_t* new_msg = (t + 1 < p.T && valid) ? p.ck_lr + ((size_t)(t + 1) * p.batch + cw) * msg_words : nullptr;
+        for (int i = zx; i < p.n; i += p.Zc) ck_lq[((size_t)t * p.batch + cw) * p.n + i] = lq[i];
+      uint32_t* old_msg = (t > 0 && valid) ? p.ck_lr + ((size_t)t * p.batch + cw) * cw_words : nullptr;
+      uint32_t* new_msg = (t + 1 < p.T && valid) ? p.ck_lr + ((size_t)(t + 1) * p.batch + cw) * cw_words : nullptr;
       __syncthreads();
       for (int row = 0; row < p.R; ++row) {
         if (valid) {
           const int e0 = p.row_off[row], deg = p.row_off[row + 1] - e0;
-          const float alpha = p.alpha[t * p.R + row], beta = p.beta[t * p.R + row];
-          NRLDPC_TRAIN_DISPATCH(train_row_fwd, deg, p, lq, (uint32_t)zx, e0, row, alpha, beta, old_msg, new_msg,
-                                nullptr)
+          const Real alpha = alpha_t[t * p.R + row], beta = beta_t[t * p.R + row];
+          NRLDPC_TRAIN_DISPATCH(train_row_fwd, Real, deg, p, lq, (uint32_t)zx, e0, row, alpha, beta, old_msg,
+                                new_msg, nullptr)
         }
         __syncthreads();
       }
-      if (valid && p.iter_llr)
-        for (int i = zx; i < p.n; i += p.Zc) p.iter_llr[((size_t)t * p.batch + cw) * p.n + i] = lq[i];
+      if (valid && iter_llr)
+        for (int i = zx; i < p.n; i += p.Zc) iter_llr[((size_t)t * p.batch + cw) * p.n + i] = lq[i];
     }
     if (valid)
-      for (int i = zx; i < p.n; i += p.Zc) p.final_llr[(size_t)cw * p.n + i] = lq[i];
+      for (int i = zx; i < p.n; i += p.Zc) final_llr[(size_t)cw * p.n + i] = lq[i];
     __syncthreads();
   }
 }
 
+template <typename Real>
 __global__ void __launch_bounds__(kThreadsTarget) train_backward_kernel(const __grid_constant__ TrainParams p) {
-  extern __shared__ __align__(16) float s_buf[];
-  __shared__ float s_red[2][2][kThreadsTarget / 32];   // [row parity][alpha, beta][warp]
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  __shared__ Real s_red[2][2][kThreadsTarget / 32];   // [row parity][alpha, beta][warp]
+  Real* s_buf = reinterpret_cast<Real*>(s_raw);
+  const Real* llr = static_cast<const Real*>(p.llr);
+  const Real* alpha_t = static_cast<const Real*>(p.alpha);
+  const Real* beta_t = static_cast<const Real*>(p.beta);
+  const Real* ck_lq = static_cast<const Real*>(p.ck_lq);
+  const Real* g_final = static_cast<const Real*>(p.g_final);
+  const Real* g_iter = static_cast<const Real*>(p.g_iter);
+  Real* g_llr = static_cast<Real*>(p.g_llr);
+  Real* g_alpha = static_cast<Real*>(p.g_alpha);
+  Real* g_beta = static_cast<Real*>(p.g_beta);
+  const Real clip = (Real)p.clip;
   const int tid = threadIdx.x;
   const int g = tid / p.Zc, zx = tid - g * p.Zc;
   const bool active = g < p.G;
-  float* lq = s_buf + (active ? g : 0) * p.n;
-  float* glq = s_buf + (size_t)p.G * p.n + (active ? g : 0) * p.n;
-  const size_t msg_words = (size_t)p.R * 4 * p.Zc;
-  const size_t edge_words = (size_t)p.nnz * p.Zc;
-  float* tape = p.tape + (size_t)blockIdx.x * p.scratch_per_cta + (size_t)(active ? g : 0) * edge_words;
-  float* carry = p.carry + (size_t)blockIdx.x * p.scratch_per_cta + (size_t)(active ? g : 0) * edge_words;
+  Real* lq = s_buf + (active ? g : 0) * p.n;
+  Real* glq = s_buf + (size_t)p.G * p.n + (active ? g : 0) * p.n;
+  const size_t cw_words = (size_t)p.R * p.msg_words;
+  const size_t edge_elems = (size_t)p.nnz * p.Zc;
+  Real* tape = static_cast<Real*>(p.tape) + (size_t)blockIdx.x * p.scratch_per_cta + (size_t)(active ? g : 0) * edge_elems;
+  Real* carry = static_cast<Real*>(p.carry) + (size_t)blockIdx.x * p.scratch_per_cta + (size_t)(active ? g : 0) * edge_elems;
   for (int item = blockIdx.x; item * p.G < p.batch; item += gridDim.x) {
     const int cw = item * p.G + g;
     const bool valid = active && cw < p.batch;
     if (valid) {
-      for (int i = zx; i < p.n; i += p.Zc) glq[i] = p.g_final ? p.g_final[(size_t)cw * p.n + i] : 0.0f;
-      for (size_t e = zx; e < edge_words; e += p.Zc) carry[e] = 0.0f;
+      for (int i = zx; i < p.n; i += p.Zc) glq[i] = g_final ? g_final[(size_t)cw * p.n + i] : (Real)0;
+      for (size_t e = zx; e < edge_elems; e += p.Zc) carry[e] = 0;
     }
     __syncthreads();
     for (int t = p.T - 1; t >= 0; --t) {
       if (valid) {
         for (int i = zx; i < p.n; i += p.Zc) {
-          lq[i] = p.ck_lq[((size_t)t * p.batch + cw) * p.n + i];
-          if (p.g_iter) glq[i] += p.g_iter[((size_t)t * p.batch + cw) * p.n + i];
+          lq[i] = ck_lq[((size_t)t * p.batch + cw) * p.n + i];
+          if (g_iter) glq[i] += g_iter[((size_t)t * p.batch + cw) * p.n + i];
         }
       }
-      const uint32_t* old_msg = (t > 0 && valid) ? p.ck_lr + ((size_t)t * p.batch + cw) * msg_words : nullptr;
+      uint32_t* old_msg = (t > 0 && valid) ? p.ck_lr + ((size_t)t * p.batch + cw) * cw_words : nullptr;
       __syncthreads();
       // Recompute iteration t, keeping every rel on the tape.
       for (int row = 0; row < p.R; ++row) {
         if (valid) {
           const int e0 = p.row_off[row], deg = p.row_off[row + 1] - e0;
-          const float alpha = p.alpha[t * p.R + row], beta = p.beta[t * p.R + row];
-          NRLDPC_TRAIN_DISPATCH(train_row_fwd, deg, p, lq, (uint32_t)zx, e0, row, alpha, beta, old_msg, nullptr,
-                                tape)
+          const Real alpha = alpha_t[t * p.R + row], beta = beta_t[t * p.R + row];
+          NRLDPC_TRAIN_DISPATCH(train_row_fwd, Real, deg, p, lq, (uint32_t)zx, e0, row, alpha, beta, old_msg,
+                                nullptr, tape)
         }
         __syncthreads();
       }
       // Back-propagate through the rows of iteration t.
       for (int row = p.R - 1; row >= 0; --row) {
-        float ga = 0.0f, gb = 0.0f;
+        Real ga = 0, gb = 0;
         if (valid) {
           const int e0 = p.row_off[row], deg = p.row_off[row + 1] - e0;
-          const float alpha = p.alpha[t * p.R + row], beta = p.beta[t * p.R + row];
-          NRLDPC_TRAIN_DISPATCH(train_row_bwd, deg, p, glq, (uint32_t)zx, e0, alpha, beta, tape, carry, &ga, &gb)
+          const Real alpha = alpha_t[t * p.R + row], beta = beta_t[t * p.R + row];
+          NRLDPC_TRAIN_DISPATCH(train_row_bwd, Real, deg, p, glq, (uint32_t)zx, e0, alpha, beta, tape, carry, &ga,
+                                &gb)
         }
         // Block-level sum of this row's alpha/beta gradient, one atomic each.
         for (int o = 16; o > 0; o >>= 1) {
@@ -292,53 +343,60 @@ __global__ void __launch_bounds__(kThreadsTarget) train_backward_kernel(const __
         }
         __syncthreads();
         if (tid == 0) {
-          float sa = 0.0f, sb = 0.0f;
+          Real sa = 0, sb = 0;
           for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
             sa += s_red[row & 1][0][w];
             sb += s_red[row & 1][1][w];
           }
-          if (sa != 0.0f) atomicAdd(p.g_alpha + t * p.R + row, sa);
-          if (sb != 0.0f) atomicAdd(p.g_beta + t * p.R + row, sb);
+          if (sa != (Real)0) atomicAdd(g_alpha + t * p.R + row, sa);
+          if (sb != (Real)0) atomicAdd(g_beta + t * p.R + row, sb);
         }
       }
     }
     if (valid)
       for (int i = zx; i < p.n; i += p.Zc) {
-        const float x = p.llr[(size_t)cw * p.n + i];
-        p.g_llr[(size_t)cw * p.n + i] = (x >= -p.clip && x <= p.clip) ? glq[i] : 0.0f;
+        const Real x = llr[(size_t)cw * p.n + i];
+        g_llr[(size_t)cw * p.n + i] = (x >= -clip && x <= clip) ? glq[i] : (Real)0;
       }
     __syncthreads();
   }
 }
 
+template <typename K>
+int launch_one(K kernel, const TrainParams& p, int grid, int block, int smem, void* stream) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return (int)e;
+  kernel<<<grid, block, smem, reinterpret_cast<cudaStream_t>(stream)>>>(p);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+template <typename K>
+int occupancy_one(K kernel, int block, int smem) {
+  int n = 0;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, smem);
+  return n;
+}
+
 }  // namespace
 
-int launch_train_forward(const TrainParams& p, int grid, int block, int smem, void* stream) {
-  cudaError_t e = cudaFuncSetAttribute(train_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return (int)e;
-  train_forward_kernel<<<grid, block, smem, reinterpret_cast<cudaStream_t>(stream)>>>(p);
-  count_launch();
-  return (int)cudaGetLastError();
+int launch_train_forward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream) {
+  return f64 ? launch_one(train_forward_kernel<double>, p, grid, block, smem, stream)
+             : launch_one(train_forward_kernel<float>, p, grid, block, smem, stream);
 }
 
-int launch_train_backward(const TrainParams& p, int grid, int block, int smem, void* stream) {
-  cudaError_t e = cudaFuncSetAttribute(train_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return (int)e;
-  train_backward_kernel<<<grid, block, smem, reinterpret_cast<cudaStream_t>(stream)>>>(p);
-  count_launch();
-  return (int)cudaGetLastError();
+int launch_train_backward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream) {
+  return f64 ? launch_one(train_backward_kernel<double>, p, grid, block, smem, stream)
+             : launch_one(train_backward_kernel<float>, p, grid, block, smem, stream);
 }
 
-int occupancy_train(bool backward, int block, int smem) {
-  int n = 0;
-  if (backward) {
-    cudaFuncSetAttribute(train_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, train_backward_kernel, block, smem);
-  } else {
-    cudaFuncSetAttribute(train_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, train_forward_kernel, block, smem);
-  }
-  return n;
+int occupancy_train(bool backward, bool f64, int block, int smem) {
+  if (backward)
+    return f64 ? occupancy_one(train_backward_kernel<double>, block, smem)
+               : occupancy_one(train_backward_kernel<float>, block, smem);
+  return f64 ? occupancy_one(train_forward_kernel<double>, block, smem)
+             : occupancy_one(train_forward_kernel<float>, block, smem);
 }
 
 }  // namespace nrldpc

@@ -115,6 +115,8 @@ def ldpc_encode(info: torch.Tensor, inconfig) -> torch.Tensor:
     cfg = _as_in_config(inconfig)
     if not info.is_cuda or info.dtype != torch.uint8 or info.dim() != 2:
         raise ValueError("info must be a uint8 CUDA tensor of shape [n, A/8]")
+    if info.shape[1] < (cfg.A + 7) // 8:
+        raise ValueError(f"info rows must hold ceil(A/8) = {(cfg.A + 7) // 8} bytes")
     if info.stride(1) != 1:
         info = info.contiguous()
     n = info.shape[0]

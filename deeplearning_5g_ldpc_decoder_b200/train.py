@@ -36,31 +36,50 @@ def _cfg(config) -> capi.LdpcInConfig:
     return capi.make_in_config(*config)
 
 
+def _vp(t: Optional[torch.Tensor]) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr() if t is not None else 0)
+
+
+def checkpoint_sizes(cfg: capi.LdpcInConfig, T: int, batch: int, f64: bool) -> Tuple[int, int]:
+    """(reals of the LQ checkpoints, uint32 words of the message checkpoints)."""
+    lib = capi.load_library()
+    lq, msg = ctypes.c_int64(0), ctypes.c_int64(0)
+    rc = lib.nrldpc_train_checkpoint_words(ctypes.byref(cfg), T, batch, int(f64), ctypes.byref(lq), ctypes.byref(msg))
+    if rc != 0:
+        raise ValueError(f"configuration not supported by the training kernels ({'float64' if f64 else 'float32'}): {rc}")
+    return int(lq.value), int(msg.value)
+
+
 class MinSumUnrolled(torch.autograd.Function):
-    """(llr [batch, n], alpha [T, R], beta [T, R]) -> (final [batch, n], per-iteration [T, batch, n])."""
+    """(llr [batch, n], alpha [T, R], beta [T, R]) -> (final [batch, n], per-iteration [T, batch, n]).
+
+    Runs in the dtype of ``llr``: float32 (training) or float64 (gradient checks)."""
 
     @staticmethod
     def forward(ctx, llr, alpha_tab, beta_tab, config, clip, detach, want_iters):
         lib = capi.load_library()
         cfg = _cfg(config)
-        llr = llr.contiguous().float()
-        alpha_tab = alpha_tab.contiguous().float()
-        beta_tab = beta_tab.contiguous().float()
+        f64 = llr.dtype == torch.float64
+        dt = torch.float64 if f64 else torch.float32
+        llr = llr.contiguous().to(dt)
+        alpha_tab = alpha_tab.contiguous().to(dt)
+        beta_tab = beta_tab.contiguous().to(dt)
         T, R = alpha_tab.shape
         batch, n = llr.shape
-        p = capi.gen_ldpc_parameters(cfg, lib)
+        if beta_tab.shape != (T, R):
+            raise ValueError("alpha and beta tables must both be [iterations, rows]")
         dev = llr.device
+        lq_elems, msg_words = checkpoint_sizes(cfg, T, batch, f64)
         final = torch.empty_like(llr)
-        iters = torch.empty((T, batch, n), dtype=torch.float32, device=dev) if want_iters else None
-        ck_lq = torch.empty((T, batch, n), dtype=torch.float32, device=dev)
-        ck_lr = torch.empty((T, batch, R * 4 * p.Zc), dtype=torch.int32, device=dev)
-        stream = torch.cuda.current_stream(dev).cuda_stream
+        iters = torch.empty((T, batch, n), dtype=dt, device=dev) if want_iters else None
+        ck_lq = torch.empty(lq_elems, dtype=dt, device=dev)
+        ck_lr = torch.empty(max(msg_words, 2), dtype=torch.int32, device=dev)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        fn = lib.nrldpc_train_forward_f64 if f64 else lib.nrldpc_train_forward
+        clip_arg = (ctypes.c_double if f64 else ctypes.c_float)(clip or INF_CLIP)
         with torch.cuda.device(dev):
-            rc = lib.nrldpc_train_forward(
-                ctypes.c_void_p(llr.data_ptr()), batch, ctypes.byref(cfg), T, ctypes.c_void_p(alpha_tab.data_ptr()),
-                ctypes.c_void_p(beta_tab.data_ptr()), ctypes.c_float(clip or INF_CLIP),
-                ctypes.c_void_p(final.data_ptr()), ctypes.c_void_p(iters.data_ptr() if iters is not None else 0),
-                ctypes.c_void_p(ck_lq.data_ptr()), ctypes.c_void_p(ck_lr.data_ptr()), ctypes.c_void_p(stream))
+            rc = fn(_vp(llr), batch, ctypes.byref(cfg), T, _vp(alpha_tab), _vp(beta_tab), clip_arg, _vp(final),
+                    _vp(iters), _vp(ck_lq), _vp(ck_lr), stream)
         if rc != 0:
             raise RuntimeError(f"nrldpc_train_forward failed: {rc}")
         ctx.save_for_backward(llr, alpha_tab, beta_tab, ck_lq, ck_lr)
@@ -68,8 +87,8 @@ class MinSumUnrolled(torch.autograd.Function):
         ctx.clip = clip
         ctx.detach = detach
         if iters is None:
-            iters = torch.empty((0,), device=dev)
-        ctx.mark_non_differentiable(iters) if not want_iters else None
+            iters = torch.empty((0,), dtype=dt, device=dev)
+            ctx.mark_non_differentiable(iters)
         return final, iters
 
     @staticmethod
@@ -77,23 +96,22 @@ class MinSumUnrolled(torch.autograd.Function):
         lib = capi.load_library()
         llr, alpha_tab, beta_tab, ck_lq, ck_lr = ctx.saved_tensors
         cfg = _cfg(ctx.cfg)
+        f64 = llr.dtype == torch.float64
         T, R = alpha_tab.shape
         batch, n = llr.shape
         dev = llr.device
         g_llr = torch.empty_like(llr)
         g_alpha = torch.zeros_like(alpha_tab)
         g_beta = torch.zeros_like(beta_tab)
-        gf = g_final.contiguous().float() if g_final is not None else None
-        gi = g_iters.contiguous().float() if (g_iters is not None and g_iters.numel() == T * batch * n) else None
-        stream = torch.cuda.current_stream(dev).cuda_stream
+        gf = g_final.contiguous().to(llr.dtype) if g_final is not None else None
+        gi = (g_iters.contiguous().to(llr.dtype)
+              if (g_iters is not None and g_iters.numel() == T * batch * n) else None)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        fn = lib.nrldpc_train_backward_f64 if f64 else lib.nrldpc_train_backward
+        clip_arg = (ctypes.c_double if f64 else ctypes.c_float)(ctx.clip or INF_CLIP)
         with torch.cuda.device(dev):
-            rc = lib.nrldpc_train_backward(
-                ctypes.c_void_p(llr.data_ptr()), batch, ctypes.byref(cfg), T, ctypes.c_void_p(alpha_tab.data_ptr()),
-                ctypes.c_void_p(beta_tab.data_ptr()), ctypes.c_float(ctx.clip or INF_CLIP), int(ctx.detach),
-                ctypes.c_void_p(ck_lq.data_ptr()), ctypes.c_void_p(ck_lr.data_ptr()),
-                ctypes.c_void_p(gf.data_ptr() if gf is not None else 0),
-                ctypes.c_void_p(gi.data_ptr() if gi is not None else 0), ctypes.c_void_p(g_llr.data_ptr()),
-                ctypes.c_void_p(g_alpha.data_ptr()), ctypes.c_void_p(g_beta.data_ptr()), ctypes.c_void_p(stream))
+            rc = fn(_vp(llr), batch, ctypes.byref(cfg), T, _vp(alpha_tab), _vp(beta_tab), clip_arg, int(ctx.detach),
+                    _vp(ck_lq), _vp(ck_lr), _vp(gf), _vp(gi), _vp(g_llr), _vp(g_alpha), _vp(g_beta), stream)
         if rc != 0:
             raise RuntimeError(f"nrldpc_train_backward failed: {rc}")
         return g_llr, g_alpha, g_beta, None, None, None, None

@@ -282,7 +282,11 @@ int32_t nrldpc_mixed_plan_destroy(void *plan);
  * Writes d_final [batch][N+2Zc], optionally every iteration's LLRs d_iter
  * [iterations][batch][N+2Zc], and the checkpoints the backward needs:
  * d_ck_lq float [iterations][batch][N+2Zc] and d_ck_lr uint32
- * [iterations][batch][rows][4][Zc].  No early termination. */
+ * [iterations][batch][rows][4 Zc] (per lifted row block: two magnitudes, the
+ * sign-flip bits and the first-minimum index of every check row; sizes from
+ * nrldpc_train_checkpoint_words).  No early termination.
+ * Forward semantics: CTableNeuralLayeredMinSumDecoder.forward,
+ * deep_learning/deeplearning_ldpc_model.py:315-410. */
 int32_t nrldpc_train_forward(const float *d_llr, int32_t batch, const ldpc_in_config_t *cfg,
                              int32_t iterations, const float *d_alpha, const float *d_beta,
                              float clip, float *d_final, float *d_iter, float *d_ck_lq,
@@ -299,6 +303,27 @@ int32_t nrldpc_train_backward(const float *d_llr, int32_t batch, const ldpc_in_c
                               const uint32_t *d_ck_lr, const float *d_g_final,
                               const float *d_g_iter, float *d_g_llr, float *d_g_alpha,
                               float *d_g_beta, void *stream);
+
+/* The same two kernels in float64, for gradient checks against finite
+ * differences (float64 needs 2 (N+2Zc) doubles of shared memory per code block:
+ * -2 where even one block does not fit, e.g. BG1 Zc > 208).  d_ck_lr is then
+ * [iterations][batch][rows][6 Zc] uint32 words. */
+int32_t nrldpc_train_forward_f64(const double *d_llr, int32_t batch, const ldpc_in_config_t *cfg,
+                                 int32_t iterations, const double *d_alpha, const double *d_beta,
+                                 double clip, double *d_final, double *d_iter, double *d_ck_lq,
+                                 uint32_t *d_ck_lr, void *stream);
+int32_t nrldpc_train_backward_f64(const double *d_llr, int32_t batch, const ldpc_in_config_t *cfg,
+                                  int32_t iterations, const double *d_alpha, const double *d_beta,
+                                  double clip, int32_t detach, const double *d_ck_lq,
+                                  const uint32_t *d_ck_lr, const double *d_g_final,
+                                  const double *d_g_iter, double *d_g_llr, double *d_g_alpha,
+                                  double *d_g_beta, void *stream);
+
+/* Checkpoint sizes of one training forward: *lq_elems reals for d_ck_lq and
+ * *msg_words uint32 words for d_ck_lr (f64 != 0: the float64 variant). */
+int32_t nrldpc_train_checkpoint_words(const ldpc_in_config_t *cfg, int32_t iterations,
+                                      int32_t batch, int32_t f64, int64_t *lq_elems,
+                                      int64_t *msg_words);
 
 /* Replace the per-(iteration, row) alpha/beta tables used by algo 2 for one
  * base graph (the reference compiles these in:

@@ -45,32 +45,38 @@ def _loss(model, llr, target, w=0.25):
 
 @pytest.mark.parametrize("name", CASES)
 def test_kernels_match_reference_model_vectors(cuda, tg, name):  # noqa: F811
-    from deeplearning_5g_ldpc_decoder_b200.train import NeuralLayeredMinSumDecoder
+    """Forward bit-exact given the reference's alpha / beta values; gradients of the
+    loss with respect to raw_alpha, raw_beta and the LLRs within float32
+    summation-order tolerance.  (torch's CUDA sigmoid may differ from its CPU
+    sigmoid in the last bit, so the forward check feeds the recorded alpha / beta.)"""
+    from deeplearning_5g_ldpc_decoder_b200.train import MinSumUnrolled, NeuralLayeredMinSumDecoder, decoder_loss
 
     c = case(tg, name)
-    m = NeuralLayeredMinSumDecoder((c["bgn"], c["A"], c["crc"], c["E"], 0, c["Qm"], 0), num_iterations=c["T"],
-                                   alpha_mode=c["mode"], clip_llr=c["clip"], detach_check_update_inputs=c["detach"],
-                                   init_beta=0.02).cuda()
+    cfg = (c["bgn"], c["A"], c["crc"], c["E"], 0, c["Qm"], 0)
+    m = NeuralLayeredMinSumDecoder(cfg, num_iterations=c["T"], alpha_mode=c["mode"], clip_llr=c["clip"],
+                                   detach_check_update_inputs=c["detach"], init_beta=0.02).cuda()
+    x = torch.tensor(tg[name + "/llr"], device=cuda)
+    a_tab = alpha_table(c["mode"], torch.tensor(tg[name + "/alpha"]), m.row_degrees, c["T"]).contiguous().cuda()
+    b_tab = torch.tensor(tg[name + "/beta"]).cuda()
+    final, its = MinSumUnrolled.apply(x, a_tab, b_tab, cfg, c["clip"], c["detach"], True)
+    assert torch.equal(final.cpu(), torch.tensor(tg[name + "/final"]))
+    assert torch.equal(its.cpu(), torch.tensor(tg[name + "/iters"]))
+    assert torch.equal((final < 0).cpu().to(torch.uint8), torch.tensor(tg[name + "/bits"]))
+
     with torch.no_grad():
         m.raw_alpha.copy_(torch.tensor(tg[name + "/raw_alpha"]))
         m.raw_beta.copy_(torch.tensor(tg[name + "/raw_beta"]))
-    x = torch.tensor(tg[name + "/llr"], device=cuda, requires_grad=True)
+    xg = x.clone().requires_grad_(True)
     tgt = torch.tensor(tg[name + "/target"], device=cuda)
-    bits, final, its = m(x, return_llr=True, return_iteration_llrs=True)
-    assert torch.equal(final.detach().cpu(), torch.tensor(tg[name + "/final"]))
-    assert torch.equal(bits.cpu().to(torch.uint8), torch.tensor(tg[name + "/bits"]))
-    for t, it in enumerate(its):
-        assert torch.equal(it.detach().cpu(), torch.tensor(tg[name + "/iters"][t]))
-    from deeplearning_5g_ldpc_decoder_b200.train import decoder_loss
-
-    loss = decoder_loss(final, tgt, m.B)
+    _, fin, it_list = m(xg, return_llr=True, return_iteration_llrs=True)
+    loss = decoder_loss(fin, tgt, m.B)
     if c["w"] > 0 and c["T"] > 1:
-        loss = loss + c["w"] * torch.stack([decoder_loss(i, tgt, m.B) for i in its[:-1]]).mean()
-    assert abs(loss.item() - float(tg[name + "/loss"][0])) < 1e-6
+        loss = loss + c["w"] * torch.stack([decoder_loss(i, tgt, m.B) for i in it_list[:-1]]).mean()
+    assert abs(loss.item() - float(tg[name + "/loss"][0])) < 1e-5
     loss.backward()
     grad_close(m.raw_alpha.grad.cpu(), tg[name + "/g_raw_alpha"])
     grad_close(m.raw_beta.grad.cpu(), tg[name + "/g_raw_beta"])
-    grad_close(x.grad.cpu(), tg[name + "/g_llr"])
+    grad_close(xg.grad.cpu(), tg[name + "/g_llr"])
 
 
 @pytest.mark.parametrize("wl", sorted(WORKLOADS))
@@ -120,78 +126,96 @@ def _set_flat(m, v):
         m.raw_beta.copy_(v[na:].reshape(m.raw_beta.shape))
 
 
-def _loss64(m, llr, target):
-    """Loss of the kernel forward, accumulated in float64."""
+def _loss_value(m, llr, target, w=0.25):
     with torch.no_grad():
-        _, final, its = m(llr, return_llr=True, return_iteration_llrs=True)
-        t = target.double()
-
-        def bce(z):
-            logits = -z[:, : m.B].double()
-            return torch.nn.functional.binary_cross_entropy_with_logits(logits, t)
-
-        return float(bce(final) + 0.25 * torch.stack([bce(i) for i in its[:-1]]).mean())
+        return float(_loss(m, llr, target, w))
 
 
-@pytest.mark.parametrize("wl,mode", [("bg2_zc64", "checkpoint"), ("bg2_zc64", "degree"), ("bg1_zc112", "single")])
-def test_gradient_vs_central_finite_differences(cuda, wl, mode):
+# Finite differences run on the float64 kernels: the min-sum loss is continuous
+# and piecewise smooth, with a kink wherever two check-row minima swap, and in
+# float32 the rounding noise at a step small enough to avoid kinks swamps the
+# difference quotient.  (The float32 kernels are tied to autograd by the tests
+# above.)  Near convergence the pieces are wide and a step of 1e-7 sees one; in
+# the low-SNR regime the gradient is large (~1e3) and the pieces narrow, so the
+# step is 1e-10 -- the difference quotient converges to the kernel's gradient as
+# the step shrinks in both regimes.
+@pytest.mark.parametrize("wl,mode,ebn0,h", [("bg2_zc64", "checkpoint", 1.5, 1e-7), ("bg2_zc64", "degree", 2.0, 1e-7),
+                                            ("bg1_zc112", "single", 1.5, 1e-7),
+                                            ("bg2_zc64", "checkpoint", 0.0, 1e-10),
+                                            ("bg2_zc64", "degree", 1.0, 1e-10)])
+def test_gradient_vs_central_finite_differences(cuda, wl, mode, ebn0, h):
     from deeplearning_5g_ldpc_decoder_b200.train import ebn0_to_noise_power_db, make_training_batch
 
     cfg = WORKLOADS[wl]
     T = 10
-    m = _model(cfg, T, mode, seed=7)
+    m = _model(cfg, T, mode, seed=7).double()
     batch = 16 if wl == "bg2_zc64" else 4
-    llr, target = make_training_batch(m, batch, ebn0_to_noise_power_db(1.5, 2, m.B, cfg[3]), seed=9)
+    llr, target = make_training_batch(m, batch, ebn0_to_noise_power_db(ebn0, 2, m.B, cfg[3]), seed=9)
+    llr, target = llr.double(), target.double()
     m.zero_grad()
-    loss = _loss(m, llr, target)
-    loss.backward()
-    g = torch.cat([m.raw_alpha.grad.reshape(-1), m.raw_beta.grad.reshape(-1)]).double().cpu()
+    _loss(m, llr, target).backward()
+    g = torch.cat([m.raw_alpha.grad.reshape(-1), m.raw_beta.grad.reshape(-1)]).cpu()
+    assert g.dtype == torch.float64 and float(g.norm()) > 0
     p0 = _flat_params(m)
-    h = 1e-3
     fd = torch.zeros_like(g)
     for i in range(p0.numel()):
         e = torch.zeros_like(p0)
         e[i] = h
         _set_flat(m, p0 + e)
-        fp = _loss64(m, llr, target)
+        fp = _loss_value(m, llr, target)
         _set_flat(m, p0 - e)
-        fm = _loss64(m, llr, target)
+        fm = _loss_value(m, llr, target)
         fd[i] = (fp - fm) / (2 * h)
     _set_flat(m, p0)
     rel = float((fd - g).norm() / g.norm())
     assert rel < 1e-3, f"norm-wise relative error {rel:.3e}"
     # a random direction through all parameters at once
-    v = torch.randn(p0.shape, generator=torch.Generator().manual_seed(1)).to(p0.device)
+    v = torch.randn(p0.shape, generator=torch.Generator().manual_seed(1), dtype=torch.float64).to(p0.device)
     v = v / v.norm()
     _set_flat(m, p0 + h * v)
-    fp = _loss64(m, llr, target)
+    fp = _loss_value(m, llr, target)
     _set_flat(m, p0 - h * v)
-    fm = _loss64(m, llr, target)
+    fm = _loss_value(m, llr, target)
     _set_flat(m, p0)
     dd = (fp - fm) / (2 * h)
-    an = float(g @ v.double().cpu())
-    assert abs(dd - an) < 1e-3 * abs(an) + 1e-9, (dd, an)
+    an = float(g @ v.cpu())
+    assert abs(dd - an) < 1e-3 * abs(an), (dd, an)
 
 
 def test_gradient_wrt_llr_finite_differences(cuda):
     from deeplearning_5g_ldpc_decoder_b200.train import ebn0_to_noise_power_db, make_training_batch
 
     cfg = WORKLOADS["bg2_zc64"]
-    m = _model(cfg, 6, "checkpoint", seed=11)
+    m = _model(cfg, 6, "checkpoint", seed=11).double()
     llr, target = make_training_batch(m, 8, ebn0_to_noise_power_db(1.0, 2, m.B, cfg[3]), seed=13)
+    llr, target = llr.double(), target.double()
     x = llr.clone().requires_grad_(True)
     _loss(m, x, target).backward()
-    gx = x.grad.double().cpu()
-    h = 1e-3
+    gx = x.grad.cpu()
+    h = 1e-7
     gen = torch.Generator().manual_seed(2)
     for _ in range(4):
-        v = torch.randn(llr.shape, generator=gen).to(llr.device)
+        v = torch.randn(llr.shape, generator=gen, dtype=torch.float64).to(llr.device)
         v = v / v.norm()
-        fp = _loss64(m, llr + h * v, target)
-        fm = _loss64(m, llr - h * v, target)
-        dd = (fp - fm) / (2 * h)
-        an = float((gx * v.double().cpu()).sum())
-        assert abs(dd - an) < 1e-3 * abs(an) + 1e-9, (dd, an)
+        dd = (_loss_value(m, llr + h * v, target) - _loss_value(m, llr - h * v, target)) / (2 * h)
+        an = float((gx * v.cpu()).sum())
+        assert abs(dd - an) < 1e-3 * abs(an), (dd, an)
+
+
+def test_float64_kernels_agree_with_float32_path(cuda):
+    """The float64 instantiation computes the same function: forwards agree to
+    float32 rounding on a well-conditioned batch."""
+    from deeplearning_5g_ldpc_decoder_b200.train import ebn0_to_noise_power_db, make_training_batch
+
+    cfg = WORKLOADS["bg2_zc64"]
+    m = _model(cfg, 4, "checkpoint", seed=5)
+    llr, _ = make_training_batch(m, 8, ebn0_to_noise_power_db(3.0, 2, m.B, cfg[3]), seed=3)
+    _, f32 = m(llr, return_llr=True)
+    m64 = _model(cfg, 4, "checkpoint", seed=5).double()
+    _, f64 = m64(llr.double(), return_llr=True)
+    assert f64.dtype == torch.float64
+    err = (f64 - f32.double()).abs().max() / f64.abs().max()
+    assert float(err) < 1e-4
 
 
 def test_learned_tables_decode_bit_exact_vs_c(cuda, oracle):
