@@ -187,6 +187,8 @@ def cpu_baseline(per_proc: int = 0, procs: int = 0) -> dict:
 def run_gpu(args, rank, world, local_rank):
     import torch
 
+    from deeplearning_5g_ldpc_decoder_b200.shard import max_over_ranks, sum_over_ranks
+
     from deeplearning_5g_ldpc_decoder_b200 import capi, ldpc_decode
     from deeplearning_5g_ldpc_decoder_b200.capi import make_decoder_config, make_in_config
 
@@ -238,11 +240,8 @@ def run_gpu(args, rank, world, local_rank):
     launch_ms = [a.elapsed_time(b) for a, b in ev]
     iters = out.iterations.cpu().numpy()
     status = out.status.cpu().numpy()
-    ms_step = total_ms / args.steps
-    if dist is not None:
-        t = torch.tensor([ms_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_step = max_over_ranks(total_ms / args.steps, dist, dev)
+    info_bits = sum_over_ranks(n_cw * A_BITS, dist, dev)
 
     # ---- realistic inputs: device-encoded code blocks through the 256QAM channel
     # near the 1e-2 BLER point; CRC early termination as in the reference ----
@@ -257,7 +256,6 @@ def run_gpu(args, rank, world, local_rank):
         e2e_ms = run_e2e(args, lib, host_llr, out, stream, barrier, dist, dev, iters, torch)
     result = None
     if rank == 0:
-        info_bits = n_cw * A_BITS * world
         value = info_bits / (ms_step * 1e-3) / 1e9
         e2e_value = info_bits / (e2e_ms * 1e-3) / 1e9
         alg = algorithmic_bytes(iters)
@@ -308,6 +306,7 @@ def run_gpu(args, rank, world, local_rank):
 
 
 def run_early_exit(args, n_cw, dev, stream, barrier, dist, torch):
+    from deeplearning_5g_ldpc_decoder_b200.shard import max_over_ranks
     from deeplearning_5g_ldpc_decoder_b200 import channel_llrs, ldpc_decode, ldpc_encode
 
     gen = torch.Generator(device=dev).manual_seed(1234)
@@ -324,11 +323,7 @@ def run_early_exit(args, n_cw, dev, stream, barrier, dist, torch):
         out = ldpc_decode(llr, CFG, ROW, out=out)
     e1.record(stream)
     barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
     ok = (out.status == 0) & (out.hardbits[:, : A_BITS // 8] == pay).all(dim=1)
     iters = out.iterations.cpu().numpy()
     world = dist.get_world_size() if dist is not None else 1
@@ -340,6 +335,7 @@ def run_early_exit(args, n_cw, dev, stream, barrier, dist, torch):
 
 
 def run_e2e(args, lib, host_llr, out, stream, barrier, dist, dev, iters, torch):
+    from deeplearning_5g_ldpc_decoder_b200.shard import max_over_ranks
     from deeplearning_5g_ldpc_decoder_b200.capi import make_decoder_config, make_in_config
 
     n_cw = host_llr.shape[0]
@@ -369,11 +365,7 @@ def run_e2e(args, lib, host_llr, out, stream, barrier, dist, dev, iters, torch):
         e2e_step()
     e1.record(stream)
     barrier()
-    e2e_ms = e0.elapsed_time(e1) / args.steps
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
     assert np.array_equal(pin_it.numpy(), iters) and np.array_equal(pin_bits.numpy(), out.hardbits.cpu().numpy())
 
     return e2e_ms
