@@ -32,6 +32,7 @@ SOURCES = [
     "nrldpc_mixed.cu",
     "nrldpc_mixed_api.cu",
     "nrldpc_noalloc.cu",
+    "nrldpc_tb.cu",
     "nrldpc_train.cu",
     "nrldpc_tables.cpp",
 ]
@@ -39,6 +40,7 @@ HEADERS = [
     "nrldpc_internal.h",
     "nrldpc_decode_common.cuh",
     "nrldpc_fixed_row.cuh",
+    "nrldpc_tb.cuh",
     "nr_base_graphs.inc",
 ]
 

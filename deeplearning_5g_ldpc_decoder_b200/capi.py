@@ -57,6 +57,41 @@ class LdpcConfig(ctypes.Structure):
     ]
 
 
+class TbDesc(ctypes.Structure):
+    """nrldpc_tb_t: one transport block of a batch (32 bytes)."""
+
+    _fields_ = [("A", ctypes.c_int32), ("G", ctypes.c_int32), ("Qm", ctypes.c_uint16), ("rv", ctypes.c_uint16),
+                ("bgn", ctypes.c_uint16), ("pad", ctypes.c_uint16), ("llr_offset", ctypes.c_int64),
+                ("out_offset", ctypes.c_int64)]
+
+
+class TbInfo(ctypes.Structure):
+    """nrldpc_tb_info_t: segmentation of one transport block."""
+
+    _fields_ = [("C", ctypes.c_int32), ("L_tb", ctypes.c_int32), ("Kp", ctypes.c_int32), ("Zc", ctypes.c_int32),
+                ("E_lo", ctypes.c_int32), ("E_hi", ctypes.c_int32), ("n_lo", ctypes.c_int32),
+                ("cb_cfg", LdpcInConfig)]
+
+
+class ServeConfig(ctypes.Structure):
+    """nrldpc_serve_cfg_t."""
+
+    _fields_ = [("max_batch_tbs", ctypes.c_int32), ("max_batch_cbs", ctypes.c_int32),
+                ("llr_budget_bytes", ctypes.c_int64), ("pipeline_depth", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("timeout_s", ctypes.c_double)]
+
+
+class ServeStats(ctypes.Structure):
+    """nrldpc_serve_stats_t."""
+
+    _fields_ = [("admitted", ctypes.c_int64), ("dropped", ctypes.c_int64), ("completed", ctypes.c_int64),
+                ("failed", ctypes.c_int64), ("batches", ctypes.c_int64), ("wall_s", ctypes.c_double),
+                ("mean_batch_tbs", ctypes.c_double)]
+
+
+NRLDPC_TB_DROPPED = -5
+
+
 def make_decoder_config(values) -> DecoderConfig:
     """Row [algo, max_iterations, alpha, beta, filling_bit_value, max_llr, min_llr]
     (scripts/ldpc_c_sim_common.py:112-122)."""
@@ -91,6 +126,17 @@ EXPORTED_SYMBOLS = (
     "nrldpc_train_checkpoint_words",
     "nrldpc_set_trained_weights",
     "nrldpc_set_degree_alpha",
+    "nrldpc_mixed_plan_create",
+    "nrldpc_mixed_plan_execute",
+    "nrldpc_mixed_plan_autotune",
+    "nrldpc_mixed_plan_destroy",
+    "nrldpc_tb_segment",
+    "nrldpc_tb_select_bg",
+    "nrldpc_tb_engine_create",
+    "nrldpc_tb_engine_destroy",
+    "nrldpc_tb_engine_decode",
+    "nrldpc_tb_engine_views",
+    "nrldpc_serve_run",
     "nrldpc_kernel_launch_count",
     "nrldpc_version",
 )
@@ -164,6 +210,22 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nrldpc_train_checkpoint_words.argtypes = [ctypes.POINTER(LdpcInConfig), i32, i32, i32,
                                                   ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
     lib.nrldpc_train_checkpoint_words.restype = i32
+    lib.nrldpc_tb_segment.argtypes = [ctypes.POINTER(TbDesc), ctypes.POINTER(TbInfo)]
+    lib.nrldpc_tb_segment.restype = i32
+    lib.nrldpc_tb_select_bg.argtypes = [i32, i32]
+    lib.nrldpc_tb_select_bg.restype = i32
+    lib.nrldpc_tb_engine_create.argtypes = [i32, i32, ctypes.POINTER(DecoderConfig), ctypes.POINTER(vp)]
+    lib.nrldpc_tb_engine_create.restype = i32
+    lib.nrldpc_tb_engine_destroy.argtypes = [vp]
+    lib.nrldpc_tb_engine_destroy.restype = i32
+    lib.nrldpc_tb_engine_decode.argtypes = [vp, vp, i32, vp, vp, vp, vp, vp]
+    lib.nrldpc_tb_engine_decode.restype = i32
+    lib.nrldpc_tb_engine_views.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                           ctypes.POINTER(vp)]
+    lib.nrldpc_tb_engine_views.restype = i32
+    lib.nrldpc_serve_run.argtypes = [vp, ctypes.POINTER(ServeConfig), vp, vp, i32, vp, vp, vp, vp,
+                                     ctypes.POINTER(ServeStats), vp]
+    lib.nrldpc_serve_run.restype = i32
     lib.nrldpc_set_trained_weights.argtypes = [ctypes.c_uint16, vp, vp, i32]
     lib.nrldpc_set_trained_weights.restype = i32
     lib.nrldpc_set_degree_alpha.argtypes = [vp]

@@ -135,6 +135,7 @@ struct MixedParams {
   const int32_t* slots;
   const MixedCw* cws;
   int32_t num_items;
+  const int32_t* num_items_dev;        // when set, the item count is read from the device (built there)
   int32_t* counter;                    // work-queue head, zeroed before each launch
   const int16_t* llr;
   uint8_t* bits;

@@ -74,11 +74,12 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
 
   const int tid = threadIdx.x;
   uint32_t* scratch = p.scratch + (int64_t)blockIdx.x * p.scratch_words;
+  const int num_items = p.num_items_dev ? *p.num_items_dev : p.num_items;
   for (;;) {
     if (tid == 0) s_item = atomicAdd(p.counter, 1);
     __syncthreads();
     const int item = s_item;
-    if (item >= p.num_items) break;
+    if (item >= num_items) break;
     const MixedItem desc = p.items[item];
     {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(p.graphs + desc.graph);

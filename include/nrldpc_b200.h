@@ -273,6 +273,99 @@ int32_t nrldpc_mixed_plan_autotune(void *plan, const int16_t *d_llr, uint8_t *d_
 
 int32_t nrldpc_mixed_plan_destroy(void *plan);
 
+/* ---- transport blocks: segmentation, batched decode, serving loop (no
+ * counterpart in the reference's C ABI, which decodes single code blocks; the
+ * segmentation formulas are TS 38.212 5.2.2 / 5.4.2.1 as restated in
+ * py5gphy/ldpc/ldpc_info.py:59-109 and py5gphy/ldpc/nr_ldpc_ratematch.py:22-45) */
+
+#define NRLDPC_TB_DROPPED (-5)   /* serving: not admitted (HBM budget exhausted) */
+
+/* One transport block: A payload bits (multiple of 8), coded into G bits
+ * (multiple of Qm, one layer) on base graph bgn.  Its G int16 LLRs start at
+ * llr_offset in the LLR arena, code block after code block in order; its A/8
+ * decoded payload bytes go to out_offset in the output arena. */
+typedef struct {
+    int32_t A;
+    int32_t G;
+    uint16_t Qm;
+    uint16_t rv;
+    uint16_t bgn;
+    uint16_t pad;
+    int64_t llr_offset;
+    int64_t out_offset;
+} nrldpc_tb_t;
+
+/* Segmentation of one transport block (host). */
+typedef struct {
+    int32_t C;          /* code blocks */
+    int32_t L_tb;       /* transport-block CRC bits (16 or 24) */
+    int32_t Kp;         /* K': information + code-block CRC bits per code block */
+    int32_t Zc;
+    int32_t E_lo, E_hi; /* code blocks 0..n_lo-1 carry E_lo coded bits, the rest E_hi */
+    int32_t n_lo;
+    ldpc_in_config_t cb_cfg;   /* per-code-block decoder configuration (E = E_lo) */
+} nrldpc_tb_info_t;
+
+/* Returns 0, or NRLDPC_ERR_CONFIG with a reason on stderr: bad A / G / Qm /
+ * bgn / rv, sizes that do not split into equal byte-aligned code blocks
+ * (TS 38.214 transport-block sizes always do), or a code block whose E does
+ * not fit 16 bits. */
+int32_t nrldpc_tb_segment(const nrldpc_tb_t *tb, nrldpc_tb_info_t *info);
+
+/* Base graph by TS 38.212 7.2.2 from A and the target code rate R (x 1024). */
+int32_t nrldpc_tb_select_bg(int32_t A, int32_t R_x1024);
+
+/* A decode engine for batches of up to max_tbs transport blocks and max_cbs
+ * code blocks, with one fixed-point decoder setting (algos 1-3).  Each batch
+ * is segmented on the device, all its code blocks decode in one persistent
+ * launch (mixed sizes, CRC early exit per code block), and the transport-block
+ * CRC and payload gather run on the device. */
+int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_decoder_cfg_t *decoder_cfg,
+                                void **engine);
+int32_t nrldpc_tb_engine_destroy(void *engine);
+
+/* Decode num_tbs transport blocks described by d_tbs (device memory) whose LLRs
+ * are in d_llr.  Writes the payload bytes of every block to d_out, d_status
+ * [num_tbs] (0 CRC pass, 1 fail, -2 bad configuration, -4 batch over the
+ * engine's capacity) and d_iterations [num_tbs] (largest code-block iteration
+ * count; nullable).  Stream-ordered, no host synchronisation. */
+int32_t nrldpc_tb_engine_decode(void *engine, const nrldpc_tb_t *d_tbs, int32_t num_tbs, const int16_t *d_llr,
+                                uint8_t *d_out, int32_t *d_status, int32_t *d_iterations, void *stream);
+
+/* Device views of the last batch's code blocks, for inspection: hard bits
+ * [max_cbs][1056] bytes, status and iterations [max_cbs], and each transport
+ * block's first code-block index [max_tbs].  Any pointer may be NULL. */
+int32_t nrldpc_tb_engine_views(void *engine, const uint8_t **d_cb_bits, const int32_t **d_cb_status,
+                               const int32_t **d_cb_iterations, const int32_t **d_tb_first_cb);
+
+/* Serving loop. */
+typedef struct {
+    int32_t max_batch_tbs;      /* transport blocks per decode batch at most */
+    int32_t max_batch_cbs;      /* code blocks per decode batch at most */
+    int64_t llr_budget_bytes;   /* HBM for the LLRs of admitted, unfinished blocks */
+    int32_t pipeline_depth;     /* batches in flight, 1..8 */
+    int32_t pad;
+    double timeout_s;           /* the run fails with NRLDPC_ERR_CUDA after this long */
+} nrldpc_serve_cfg_t;
+
+typedef struct {
+    int64_t admitted, dropped, completed, failed, batches;
+    double wall_s;              /* first arrival to last verdict */
+    double mean_batch_tbs;
+} nrldpc_serve_stats_t;
+
+/* Run the arrival trace tbs[i] / arrival_s[i] (host arrays, arrival times in
+ * seconds from the start of the call, ascending) through the engine with
+ * continuous batching: a block is admitted on arrival if its LLR bytes fit the
+ * budget (else dropped: status NRLDPC_TB_DROPPED), admitted blocks form a new
+ * batch whenever fewer than pipeline_depth batches are in flight, and each
+ * block's verdict time is taken when its batch's completion event is observed.
+ * Writes h_status [n] and h_latency_s [n] (verdict - arrival; NaN if dropped).
+ * All waits are host polls bounded by timeout_s; no device-side waits. */
+int32_t nrldpc_serve_run(void *engine, const nrldpc_serve_cfg_t *cfg, const nrldpc_tb_t *tbs,
+                         const double *arrival_s, int32_t n, const int16_t *d_llr, uint8_t *d_out,
+                         int32_t *h_status, double *h_latency_s, nrldpc_serve_stats_t *stats, void *stream);
+
 /* ---- differentiable unrolled float min-sum (no counterpart in the reference's
  * C ABI; the training model it serves is deep_learning/deeplearning_ldpc_model.py) */
 
