@@ -131,6 +131,9 @@ struct DeviceState {
   // host-buffer batched API
   struct HostStage {
     Buffer llr, bits, stat, iters;
+    cudaStream_t copy = nullptr, comp = nullptr;   // copy engine / decode streams of the pipeline
+    cudaEvent_t start = nullptr;
+    std::vector<cudaEvent_t> h2d, dec;             // per chunk
   };
   std::map<cudaStream_t, HostStage> host_stage;
   std::map<cudaStream_t, Buffer> scratch;
@@ -656,24 +659,71 @@ int32_t nrldpc_decode_batch_host(const int16_t* h_llr, int64_t llr_stride, int32
   if (ensure(&hs.llr, llr_bytes) || ensure(&hs.bits, bit_bytes) || ensure(&hs.stat, sizeof(int32_t) * num_cw) ||
       ensure(&hs.iters, sizeof(int32_t) * num_cw))
     return NRLDPC_ERR_CUDA;
-  if (cudaMemcpyAsync(hs.llr.ptr, h_llr, llr_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+  if (!hs.copy) {
+    if (cudaStreamCreateWithFlags(&hs.copy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&hs.comp, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&hs.start, cudaEventDisableTiming) != cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+  }
+  // Chunks of whole waves of the decode kernel: chunk k+1's host-to-device copy
+  // overlaps chunk k's decode, and the waves of the chunks add up to the waves of
+  // one launch over the whole batch, so nothing is lost to partial waves.
+  Plan probe;
+  if (make_plan(cp, *decoder_cfg, num_cw, st, &probe) != 0) return NRLDPC_ERR_CUDA;
+  const bool fixed = decoder_cfg->algo >= 1 && decoder_cfg->algo <= 3;
+  const int64_t wave_cw = (int64_t)(fixed ? 2 : 1) * probe.p.G * probe.grid;
+  int64_t chunk = num_cw;
+  constexpr int kChunks = 5;
+  if (wave_cw > 0 && num_cw >= 3 * wave_cw) {
+    const int64_t want = (num_cw + kChunks - 1) / kChunks;
+    chunk = (want + wave_cw - 1) / wave_cw * wave_cw;
+  }
+  const int nchunks = (int)((num_cw + chunk - 1) / chunk);
+  while ((int)hs.h2d.size() < nchunks) {
+    cudaEvent_t a, b;
+    if (cudaEventCreateWithFlags(&a, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b, cudaEventDisableTiming) != cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+    hs.h2d.push_back(a);
+    hs.dec.push_back(b);
+  }
+  // work already queued on the caller's stream comes first
+  if (cudaEventRecord(hs.start, s) != cudaSuccess || cudaStreamWaitEvent(hs.copy, hs.start, 0) != cudaSuccess ||
+      cudaStreamWaitEvent(hs.comp, hs.start, 0) != cudaSuccess)
     return NRLDPC_ERR_CUDA;
-  int32_t rc = decode_batch_locked(static_cast<int16_t*>(hs.llr.ptr), llr_stride, num_cw, inconfig, decoder_cfg,
-                                   static_cast<uint8_t*>(hs.bits.ptr), bits_stride,
-                                   static_cast<int32_t*>(hs.stat.ptr), static_cast<int32_t*>(hs.iters.ptr), nullptr,
-                                   0, nullptr, 0, stream);
-  if (rc != NRLDPC_OK) return rc;
-  if (decoder_cfg->max_iterations > 0 &&
-      cudaMemcpyAsync(h_hardbits, hs.bits.ptr, bit_bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
-    return NRLDPC_ERR_CUDA;
-  if (h_status &&
-      cudaMemcpyAsync(h_status, hs.stat.ptr, sizeof(int32_t) * num_cw, cudaMemcpyDeviceToHost, s) != cudaSuccess)
-    return NRLDPC_ERR_CUDA;
-  if (h_iterations &&
-      cudaMemcpyAsync(h_iterations, hs.iters.ptr, sizeof(int32_t) * num_cw, cudaMemcpyDeviceToHost, s) !=
-          cudaSuccess)
-    return NRLDPC_ERR_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return NRLDPC_ERR_CUDA;
+  int16_t* d_llr = static_cast<int16_t*>(hs.llr.ptr);
+  uint8_t* d_bits = static_cast<uint8_t*>(hs.bits.ptr);
+  int32_t* d_stat = static_cast<int32_t*>(hs.stat.ptr);
+  int32_t* d_iters = static_cast<int32_t*>(hs.iters.ptr);
+  for (int k = 0; k < nchunks; ++k) {
+    const int64_t c0 = k * chunk, n = std::min<int64_t>(chunk, num_cw - c0);
+    const size_t off = (size_t)c0 * (size_t)llr_stride;
+    if (cudaMemcpyAsync(d_llr + off, h_llr + off, sizeof(int16_t) * (size_t)n * (size_t)llr_stride,
+                        cudaMemcpyHostToDevice, hs.copy) != cudaSuccess ||
+        cudaEventRecord(hs.h2d[k], hs.copy) != cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+  }
+  for (int k = 0; k < nchunks; ++k) {
+    const int64_t c0 = k * chunk, n = std::min<int64_t>(chunk, num_cw - c0);
+    if (cudaStreamWaitEvent(hs.comp, hs.h2d[k], 0) != cudaSuccess) return NRLDPC_ERR_CUDA;
+    const int32_t rc = decode_batch_locked(d_llr + (size_t)c0 * (size_t)llr_stride, llr_stride, (int32_t)n, inconfig,
+                                           decoder_cfg, d_bits + (size_t)c0 * (size_t)bits_stride, bits_stride,
+                                           d_stat + c0, d_iters + c0, nullptr, 0, nullptr, 0, hs.comp);
+    if (rc != NRLDPC_OK) return rc;
+    if (cudaEventRecord(hs.dec[k], hs.comp) != cudaSuccess || cudaStreamWaitEvent(hs.copy, hs.dec[k], 0) != cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+    if (decoder_cfg->max_iterations > 0 &&
+        cudaMemcpyAsync(h_hardbits + (size_t)c0 * (size_t)bits_stride, d_bits + (size_t)c0 * (size_t)bits_stride,
+                        (size_t)n * (size_t)bits_stride, cudaMemcpyDeviceToHost, hs.copy) != cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+    if (h_status && cudaMemcpyAsync(h_status + c0, d_stat + c0, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost,
+                                    hs.copy) != cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+    if (h_iterations && cudaMemcpyAsync(h_iterations + c0, d_iters + c0, sizeof(int32_t) * (size_t)n,
+                                        cudaMemcpyDeviceToHost, hs.copy) != cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+  }
+  if (cudaStreamSynchronize(hs.copy) != cudaSuccess) return NRLDPC_ERR_CUDA;
   return NRLDPC_OK;
 }
 

@@ -160,3 +160,27 @@ def test_algo2_beyond_table_reuses_last_row(oracle, cuda):
     cfg = (1, 1000, 1, 3000, 0, 2, 0)
     llr, _ = make_llrs(oracle, in_config(*cfg), 2, noise_db=6.0, seed=2)
     run_and_compare(oracle, cuda, cfg, [2, 40, 0, 0, 1280, 32767, -32767], llr, tag="algo2 40 it")
+
+
+@pytest.mark.parametrize("algo", [1, 4])
+def test_host_buffer_pipeline_matches_device_path(oracle, cuda, algo):
+    """nrldpc_decode_batch_host copies and decodes in overlapped chunks of whole
+    kernel waves; results equal the device-pointer path for batches below,
+    at and well above the chunking threshold, and a sample equals the oracle."""
+    from deeplearning_5g_ldpc_decoder_b200 import ldpc_decode_host
+
+    cfg = (2, 488, 1, 1920, 0, 2, 0)
+    base, _ = make_llrs(oracle, in_config(*cfg), 64, noise_db=-1.0, seed=31)
+    rng = np.random.default_rng(4)
+    row = [algo, 8, 22936, 0, 1280, 32767, -32767]
+    for n in (1, 7, 300, 4000, 13001):
+        llr = base[rng.integers(0, 64, n)]
+        llr = np.clip(llr.astype(np.int32) + rng.integers(-300, 300, llr.shape), -32767, 32767).astype(np.int16)
+        bits, st, it = ldpc_decode_host(llr, cfg, row)
+        ref = ldpc_decode(torch.from_numpy(llr).to(cuda), cfg, row)
+        assert np.array_equal(st, ref.status.cpu().numpy()), n
+        assert np.array_equal(it, ref.iterations.cpu().numpy()), n
+        assert np.array_equal(bits, ref.hardbits.cpu().numpy()), n
+        for i in rng.integers(0, n, 3):
+            es, eb, ei, _ = oracle.decode(llr[i], in_config(*cfg), dec_cfg(row))
+            assert (st[i], it[i]) == (es, ei) and np.array_equal(bits[i], eb)
