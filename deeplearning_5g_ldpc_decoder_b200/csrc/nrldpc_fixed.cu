@@ -73,6 +73,8 @@ template <bool kDegenClip>
 __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __grid_constant__ DecodeParams p) {
   extern __shared__ __align__(16) uint32_t s_lq[];        // [G][lq_len] int16x2
   __shared__ uint32_t s_crc[2 * kMaxGroups];
+  __shared__ uint2 s_edges[kMaxNnz];   // per-edge (col*Zc*4, (V mod Zc)*4), read with warp-uniform indices
+  for (int e = threadIdx.x; e < kMaxNnz; e += blockDim.x) s_edges[e] = p.edge_cs4[e];
 
   const int tid = threadIdx.x;
   const int g = tid / p.Zc;
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
                                               : p.w_inline[row];
           const int32_t alpha = (int32_t)(int16_t)(ab & 0xFFFFu);
           const int32_t beta = ((int32_t)ab) >> 16;
-          layer_dispatch<kDegenClip, false>(deg, p, nullptr, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0, alpha, beta,
+          layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0, alpha, beta,
                                      it == 0, scratch + p.lr_off[row] + tid);
         }
         __syncthreads();
