@@ -50,11 +50,12 @@ WORKLOAD = ("BG1 Zc=384 A=8424 B=8448 E=25344 (Qm=8 length, R=1/3), algo 1 int16
             "alpha=22936, 8 iterations (CRC never passes: all 8 run), 8192 code blocks per launch")
 
 
-def algorithmic_bytes(iters: np.ndarray) -> float:
+def algorithmic_bytes(iters: np.ndarray, E: int = E, fp: bool = False) -> float:
     """2E + ceil(B/8) + 4 + I_exec * (8*nnz*Zc + 2*B) per code block: every edge
-    reads LQ and Lr and writes both (int16), plus the B hard-decision reads."""
+    reads LQ and Lr and writes both (int16), plus the B hard-decision reads.
+    Float decoders (algos 0, 4) move 4-byte values: I_exec * (16*nnz*Zc + 4*B)."""
     io = 2 * E + (B_BITS + 7) // 8 + 4
-    per_it = 8 * NNZ * ZC + 2 * B_BITS
+    per_it = (16 * NNZ * ZC + 4 * B_BITS) if fp else (8 * NNZ * ZC + 2 * B_BITS)
     return float(io * len(iters) + per_it * int(np.sum(iters)))
 
 
@@ -246,8 +247,10 @@ def run_gpu(args, rank, world, local_rank):
     # ---- realistic inputs: device-encoded code blocks through the 256QAM channel
     # near the 1e-2 BLER point; CRC early termination as in the reference ----
     early = None
+    variants = None
     if not args.no_e2e:
         early = run_early_exit(args, n_cw, dev, stream, barrier, dist, torch)
+        variants = run_config2_variants(args, n_cw, dev, stream, barrier, dist, torch)
 
     # ---- end to end through the host-buffer C ABI (pinned memory) ----
     if args.no_e2e:
@@ -294,6 +297,7 @@ def run_gpu(args, rank, world, local_rank):
             "iterations_executed_mean": float(np.mean(iters)),
             "converged": int(np.sum(status == 0)),
             "early_exit": early,
+            "config2_variants": variants,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
@@ -305,33 +309,71 @@ def run_gpu(args, rank, world, local_rank):
     return result
 
 
-def run_early_exit(args, n_cw, dev, stream, barrier, dist, torch):
+def _esn0_for_bler(cfg, row, Qm, target, dev, torch, n_cw: int = 2048, lo: float = 0.0, hi: float = 35.0):
+    """Es/N0 (dB) where the block error rate of device-encoded blocks through the
+    device channel crosses `target` (bisection, 10 steps)."""
+    from deeplearning_5g_ldpc_decoder_b200 import channel_llrs, ldpc_decode, ldpc_encode
+
+    gen = torch.Generator(device=dev).manual_seed(77)
+    pay = torch.randint(0, 256, (n_cw, cfg[1] // 8), dtype=torch.uint8, device=dev, generator=gen)
+    rm = ldpc_encode(pay, cfg)
+    for k in range(10):
+        mid = 0.5 * (lo + hi)
+        res = ldpc_decode(channel_llrs(rm, cfg[3], Qm, -mid, seed=500 + k), cfg, row)
+        ok = (res.status == 0) & (res.hardbits[:, : cfg[1] // 8] == pay).all(dim=1)
+        if 1.0 - float(ok.float().mean()) > target:
+            lo = mid
+        else:
+            hi = mid
+    return round(0.5 * (lo + hi), 2)
+
+
+def run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, cfg=None, row=None, esn0=None):
+    """Realistic inputs: device-encoded payloads through the 256QAM channel at the
+    given Es/N0, CRC early termination as in the reference."""
     from deeplearning_5g_ldpc_decoder_b200.shard import max_over_ranks
     from deeplearning_5g_ldpc_decoder_b200 import channel_llrs, ldpc_decode, ldpc_encode
 
+    cfg = cfg or CFG
+    row = row or ROW
+    esn0 = ESN0_1E2_DB if esn0 is None else esn0
     gen = torch.Generator(device=dev).manual_seed(1234)
     pay = torch.randint(0, 256, (n_cw, A_BITS // 8), dtype=torch.uint8, device=dev, generator=gen)
-    llr = channel_llrs(ldpc_encode(pay, CFG), E, 8, noise_power_db=-ESN0_1E2_DB, seed=99)
+    llr = channel_llrs(ldpc_encode(pay, cfg), cfg[3], 8, noise_power_db=-esn0, seed=99)
     out = None
     for _ in range(max(args.warmup, 1)):
-        out = ldpc_decode(llr, CFG, ROW, out=out)
+        out = ldpc_decode(llr, cfg, row, out=out)
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        out = ldpc_decode(llr, CFG, ROW, out=out)
+        out = ldpc_decode(llr, cfg, row, out=out)
     e1.record(stream)
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
     ok = (out.status == 0) & (out.hardbits[:, : A_BITS // 8] == pay).all(dim=1)
     iters = out.iterations.cpu().numpy()
     world = dist.get_world_size() if dist is not None else 1
+    fp = row[0] in (0, 4)
     return {"value": round(n_cw * A_BITS * world / (ms * 1e-3) / 1e9, 4), "unit": "Gbit/s", "ms_per_step": round(ms, 4),
             "iterations_executed_mean": float(np.mean(iters)), "bler": float(1.0 - ok.float().mean().item()),
-            "roofline_achieved_gbs": round(algorithmic_bytes(iters) / (ms * 1e-3) / 1e9, 1),
-            "inputs": f"device-encoded random payloads, 256QAM AWGN at Es/N0 {ESN0_1E2_DB} dB, max-log LLRs "
-                      "quantised like the reference channel"}
+            "roofline_achieved_gbs": round(algorithmic_bytes(iters, E=cfg[3], fp=fp) / (ms * 1e-3) / 1e9, 1),
+            "inputs": f"device-encoded random payloads, E={cfg[3]}, 256QAM AWGN at Es/N0 {esn0} dB, max-log LLRs "
+                      "quantised like the reference channel",
+            "decoder": {0: "algo 0 float BP", 1: "algo 1 int16 min-sum", 4: "algo 4 float min-sum"}.get(row[0], str(row[0]))}
+
+
+def run_config2_variants(args, n_cw, dev, stream, barrier, dist, torch):
+    """The other legs of the large single-size batch: E=9600 (rate 0.88) with algo 1,
+    and algo 0 (float BP) at E=25344, each at its measured ~1e-2 BLER point."""
+    cfg88 = (1, 8424, 1, 9600, 0, 8, 0)
+    row_bp = [0, 8, 22936, 0, 1280, 32767, -32767]
+    esn0_88 = _esn0_for_bler(cfg88, ROW, 8, 0.01, dev, torch)
+    esn0_bp = _esn0_for_bler(CFG, row_bp, 8, 0.01, dev, torch, n_cw=1024, lo=5.0, hi=15.0)
+    out = {"E9600_algo1": run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, cfg88, ROW, esn0_88),
+           "E25344_algo0_bp": run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, CFG, row_bp, esn0_bp)}
+    return out
 
 
 def run_e2e(args, lib, host_llr, out, stream, barrier, dist, dev, iters, torch):

@@ -79,3 +79,50 @@ def test_noise_only_runs_every_iteration(cuda):
     torch.cuda.synchronize()
     assert (res.status.cpu() == 1).all()
     assert (res.iterations.cpu() == 8).all()
+
+
+def _device_blocks(cuda, cfg, n, esn0_db, seed):
+    from deeplearning_5g_ldpc_decoder_b200 import channel_llrs, ldpc_encode
+
+    gen = torch.Generator(device=cuda).manual_seed(seed)
+    pay = torch.randint(0, 256, (n, cfg[1] // 8), dtype=torch.uint8, device=cuda, generator=gen)
+    llr = channel_llrs(ldpc_encode(pay, cfg), cfg[3], cfg[5], -esn0_db, seed=seed)
+    return pay, llr
+
+
+def test_high_rate_full_batch(oracle, cuda):
+    """E = 9600 (rate 0.88, 256QAM) on 8192 blocks: passing blocks carry the sent
+    payload, a sample of passing and failing blocks equals the oracle exactly."""
+    cfg = (1, 8424, 1, 9600, 0, 8, 0)
+    pay, llr = _device_blocks(cuda, cfg, N_CW, 23.5, 41)
+    res = ldpc_decode(llr, cfg, ROW, return_app=True)
+    st, bits = res.status.cpu().numpy(), res.hardbits.cpu().numpy()
+    conv = np.nonzero(st == 0)[0]
+    fail = np.nonzero(st != 0)[0]
+    assert len(conv) > N_CW // 4
+    assert np.array_equal(bits[conv, : 8424 // 8], pay.cpu().numpy()[conv])
+    llr_h, app, its = llr.cpu().numpy(), res.app.cpu().numpy(), res.iterations.cpu().numpy()
+    for i in list(conv[:4]) + list(fail[:4]):
+        es, eb, ei, elq = oracle.decode(llr_h[i], in_config(*cfg), dec_cfg(ROW))
+        assert (st[i], its[i]) == (es, ei) and np.array_equal(bits[i], eb) and np.array_equal(app[i], elq), i
+
+
+def test_bp_full_size_blocks(oracle, cuda):
+    """Algo 0 (float BP) on BG1 Zc=384 blocks at E = 25344: hard bits, status and
+    iteration counts equal the oracle; beliefs within the BP tolerance."""
+    from golden_cases import lq_close
+
+    row = [0, 8, 22936, 0, 1280, 32767, -32767]
+    pay, llr = _device_blocks(cuda, CFG, 1024, 10.5, 42)
+    res = ldpc_decode(llr, CFG, row, return_app=True)
+    st, bits = res.status.cpu().numpy(), res.hardbits.cpu().numpy()
+    conv = np.nonzero(st == 0)[0]
+    assert len(conv) > 256
+    assert np.array_equal(bits[conv, : 8424 // 8], pay.cpu().numpy()[conv])
+    llr_h, app, its = llr.cpu().numpy(), res.app.cpu().numpy(), res.iterations.cpu().numpy()
+    for i in list(conv[:3]) + list(np.nonzero(st != 0)[0][:3]):
+        es, eb, ei, elq = oracle.decode(llr_h[i], in_config(*CFG), dec_cfg(row))
+        assert (st[i], its[i]) == (es, ei), i
+        if ei > 0:
+            assert np.array_equal(bits[i], eb), i
+        assert lq_close(app[i], elq, 0, es == 0), i
