@@ -44,11 +44,10 @@ BP_TIGHT_FRAC = 1e-2
 def lq_close(a: np.ndarray, b: np.ndarray, algo: int, converged: bool = True) -> bool:
     """Final-belief comparison: exact for every algorithm except BP (algo 0).
 
-    BP evaluates tanh/atanh in double precision and rounds to float, while the
-    reference calls the host libm's tanhf/atanhf; the two differ by an ulp now
-    and then and layered BP amplifies that a little.  Measured on the golden
-    vectors: p99 relative error <= 1.3e-6, max 1.4e-4 on <= 0.06% of LLRs, hard
-    decisions / status / iteration counts identical."""
+    BP calls tanhf/atanhf: CUDA's float functions on the device, the host
+    libm's in the reference; they differ by an ulp or two now and then and
+    layered BP amplifies that a little.  Hard decisions, status and iteration
+    counts are compared exactly elsewhere."""
     if algo != 0:
         return bool(np.array_equal(a, b))
     if not converged:

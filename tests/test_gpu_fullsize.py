@@ -94,7 +94,7 @@ def test_high_rate_full_batch(oracle, cuda):
     """E = 9600 (rate 0.88, 256QAM) on 8192 blocks: passing blocks carry the sent
     payload, a sample of passing and failing blocks equals the oracle exactly."""
     cfg = (1, 8424, 1, 9600, 0, 8, 0)
-    pay, llr = _device_blocks(cuda, cfg, N_CW, 23.5, 41)
+    pay, llr = _device_blocks(cuda, cfg, N_CW, 24.5, 41)
     res = ldpc_decode(llr, cfg, ROW, return_app=True)
     st, bits = res.status.cpu().numpy(), res.hardbits.cpu().numpy()
     conv = np.nonzero(st == 0)[0]
