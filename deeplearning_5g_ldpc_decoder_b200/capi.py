@@ -61,8 +61,9 @@ class TbDesc(ctypes.Structure):
     """nrldpc_tb_t: one transport block of a batch (32 bytes)."""
 
     _fields_ = [("A", ctypes.c_int32), ("G", ctypes.c_int32), ("Qm", ctypes.c_uint16), ("rv", ctypes.c_uint16),
-                ("bgn", ctypes.c_uint16), ("pad", ctypes.c_uint16), ("llr_offset", ctypes.c_int64),
-                ("out_offset", ctypes.c_int64)]
+                ("bgn", ctypes.c_uint16), ("flags", ctypes.c_uint16), ("llr_offset", ctypes.c_int64),
+                ("out_offset", ctypes.c_int64), ("tbs_lbrm", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("harq_offset", ctypes.c_int64)]
 
 
 class TbInfo(ctypes.Structure):
@@ -70,7 +71,8 @@ class TbInfo(ctypes.Structure):
 
     _fields_ = [("C", ctypes.c_int32), ("L_tb", ctypes.c_int32), ("Kp", ctypes.c_int32), ("Zc", ctypes.c_int32),
                 ("E_lo", ctypes.c_int32), ("E_hi", ctypes.c_int32), ("n_lo", ctypes.c_int32),
-                ("cb_cfg", LdpcInConfig)]
+                ("cb_cfg", LdpcInConfig), ("Ncb", ctypes.c_int32), ("k0", ctypes.c_int32),
+                ("harq_elems", ctypes.c_int64)]
 
 
 class ServeConfig(ctypes.Structure):
@@ -90,6 +92,8 @@ class ServeStats(ctypes.Structure):
 
 
 NRLDPC_TB_DROPPED = -5
+NRLDPC_TB_HARQ_COMBINE = 1
+NRLDPC_TB_HARQ_STORE = 2
 
 
 def make_decoder_config(values) -> DecoderConfig:
@@ -114,6 +118,7 @@ EXPORTED_SYMBOLS = (
     "calculate_crc",
     "tx_rx_process",
     "nrldpc_encode_batch",
+    "nrldpc_encode_batch_ncb",
     "nrldpc_channel_batch",
     "nrldpc_channel_seed",
     "nrldpc_decode_batch",
@@ -210,6 +215,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nrldpc_train_checkpoint_words.argtypes = [ctypes.POINTER(LdpcInConfig), i32, i32, i32,
                                                   ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
     lib.nrldpc_train_checkpoint_words.restype = i32
+    lib.nrldpc_encode_batch_ncb.argtypes = [vp, i64, i32, ctypes.POINTER(LdpcInConfig), i32, vp, i64, vp]
+    lib.nrldpc_encode_batch_ncb.restype = i32
     lib.nrldpc_tb_segment.argtypes = [ctypes.POINTER(TbDesc), ctypes.POINTER(TbInfo)]
     lib.nrldpc_tb_segment.restype = i32
     lib.nrldpc_tb_select_bg.argtypes = [i32, i32]
@@ -218,7 +225,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nrldpc_tb_engine_create.restype = i32
     lib.nrldpc_tb_engine_destroy.argtypes = [vp]
     lib.nrldpc_tb_engine_destroy.restype = i32
-    lib.nrldpc_tb_engine_decode.argtypes = [vp, vp, i32, vp, vp, vp, vp, vp]
+    lib.nrldpc_tb_engine_decode.argtypes = [vp, vp, i32, vp, vp, vp, vp, vp, vp]
     lib.nrldpc_tb_engine_decode.restype = i32
     lib.nrldpc_tb_engine_views.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                            ctypes.POINTER(vp)]

@@ -776,6 +776,37 @@ int32_t nrldpc_encode_batch(const uint8_t* d_info, int64_t info_stride, int32_t 
   return launch_encode(e, stream) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
 }
 
+int32_t nrldpc_encode_batch_ncb(const uint8_t* d_info, int64_t info_stride, int32_t num_cw,
+                                const ldpc_in_config_t* inconfig, int32_t ncb, uint8_t* d_rm, int64_t rm_stride,
+                                void* stream) {
+  if (!inconfig || num_cw < 0) return NRLDPC_ERR_ARG;
+  CodeParams cp;
+  if (derive_params(*inconfig, &cp, true) != 0) return NRLDPC_ERR_CONFIG;
+  if (ncb > 0 && ncb < cp.N) {
+    if (ncb < cp.K - 2 * cp.Zc) return NRLDPC_ERR_CONFIG;
+    // TS 38.212 Table 5.4.2.1-2 with Ncb < N
+    static const int fa[4] = {0, 17, 33, 56}, fb[4] = {0, 13, 25, 43};
+    const int f = (cp.bgn == 1 ? fa : fb)[cp.rv];
+    cp.k0 = (int)(((int64_t)f * ncb) / ((int64_t)(cp.bgn == 1 ? 66 : 50) * cp.Zc)) * cp.Zc;
+    cp.Nv = ncb - cp.F;
+    const int fill_lo = cp.B - 2 * cp.Zc, fill_hi = cp.K - 2 * cp.Zc;
+    cp.c0 = cp.k0 < fill_lo ? cp.k0 : (cp.k0 < fill_hi ? fill_lo : cp.k0 - cp.F);
+  }
+  if (num_cw == 0) return NRLDPC_OK;
+  if (!d_info || !d_rm || info_stride < cp.A / 8 || rm_stride < (cp.E + 7) / 8) return NRLDPC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState* st = nullptr;
+  if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
+  EncodeParams e;
+  make_encode_params(cp, st, &e);
+  e.num_cw = num_cw;
+  e.info = d_info;
+  e.info_stride = info_stride;
+  e.rm = d_rm;
+  e.rm_stride = rm_stride;
+  return launch_encode(e, stream) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
+}
+
 int32_t cuda_ldpc_5g_encode(uint8_t* infobytes, uint8_t* rm_bytes, ldpc_in_config_t* inconfig) {
   return encode_one(infobytes, rm_bytes, inconfig);
 }

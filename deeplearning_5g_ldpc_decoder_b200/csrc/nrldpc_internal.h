@@ -124,6 +124,9 @@ struct MixedCw {
   int32_t B, E, Qm, symbols, c0, Nv, F, crctype;
   int64_t llr_off;    // elements into the LLR arena
   int64_t bits_off;   // bytes into the hard-bit arena
+  int32_t ncb;        // circular-buffer length (N unless limited-buffer rate matching)
+  int32_t harq_mode;  // bit 0: add to the stored soft buffer, bit 1: store the soft buffer
+  int64_t harq_off;   // elements into the soft-buffer arena (N + 2Zc of them), when harq_mode != 0
 };
 // One work item: up to G pairs of one (BG, Zc); slots[slot_base + 2g + h] = block or -1.
 struct MixedItem {
@@ -141,6 +144,7 @@ struct MixedParams {
   uint8_t* bits;
   int32_t* status;
   int32_t* iters;
+  int16_t* harq;                       // soft-buffer arena of the blocks with harq_mode != 0 (nullable)
   const uint32_t* crc_tab;             // [4][kMaxB]
   uint32_t* scratch;
   int64_t scratch_words;               // per CTA

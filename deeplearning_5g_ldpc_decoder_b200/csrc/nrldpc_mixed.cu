@@ -23,17 +23,21 @@ namespace {
 using namespace fixedrow;
 
 // Rate recovery of soft-buffer position i of one block (c_lib/ldpc_rate_recovery.c:24-65,
-// gather form; see recover_position in nrldpc_decode_common.cuh).
+// gather form; see recover_position in nrldpc_decode_common.cuh), starting from
+// `init` (the stored soft buffer when combining a retransmission).  With a
+// limited circular buffer (ncb < N) positions at or beyond ncb take no coded
+// bits and the compacted buffer has ncb - F positions (TS 38.212 5.4.2.1).
 __device__ __forceinline__ int32_t mixed_recover(const MixedGraph& g, const MixedCw& c, const int16_t* __restrict__ in,
-                                                 int i, int32_t fill) {
+                                                 int i, int32_t fill, int32_t init) {
   const int twoZ = 2 * g.Zc;
   if (i >= c.B && i < g.K) return fill;
-  if (i < twoZ) return 0;
+  int32_t s = init;
+  if (i < twoZ) return s;
   const int pos = i - twoZ;
+  if (pos >= c.ncb) return s;
   const int cc = pos < c.B - twoZ ? pos : pos - c.F;
   int kf = cc - c.c0;
   if (kf < 0) kf += c.Nv;
-  int32_t s = 0;
   for (int k = kf; k < c.E; k += c.Nv) {
     const int b = k / c.symbols;
     const int sidx = k - b * c.symbols;
@@ -104,9 +108,15 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
     if (active) {
       const int16_t* in0 = p.llr + c0.llr_off;
       const int16_t* in1 = p.llr + c1.llr_off;
+      int16_t* h0 = (v0 && c0.harq_mode && p.harq) ? p.harq + c0.harq_off : nullptr;
+      int16_t* h1 = (v1 && c1.harq_mode && p.harq) ? p.harq + c1.harq_off : nullptr;
       for (int i = zx; i < lq_len; i += Zc) {
-        const int32_t a0 = v0 ? mixed_recover(s_g, c0, in0, i, p.fill) : 0;
-        const int32_t a1 = v1 ? mixed_recover(s_g, c1, in1, i, p.fill) : 0;
+        const int32_t i0 = (h0 && (c0.harq_mode & 1)) ? h0[i] : 0;
+        const int32_t i1 = (h1 && (c1.harq_mode & 1)) ? h1[i] : 0;
+        const int32_t a0 = v0 ? mixed_recover(s_g, c0, in0, i, p.fill, i0) : 0;
+        const int32_t a1 = v1 ? mixed_recover(s_g, c1, in1, i, p.fill, i1) : 0;
+        if (h0 && (c0.harq_mode & 2)) h0[i] = (int16_t)a0;
+        if (h1 && (c1.harq_mode & 2)) h1[i] = (int16_t)a1;
         lq[i] = ((uint32_t)a0 & 0xFFFFu) | ((uint32_t)a1 << 16);
       }
     }

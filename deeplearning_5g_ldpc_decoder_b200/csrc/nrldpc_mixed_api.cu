@@ -253,6 +253,9 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
     c.crctype = cp.crctype;
     c.llr_off = blocks[i].llr_offset;
     c.bits_off = blocks[i].bits_offset;
+    c.ncb = cp.N;
+    c.harq_mode = 0;
+    c.harq_off = 0;
   }
   MixedParams& p = pl->params;
   p.max_it = dc->max_iterations;

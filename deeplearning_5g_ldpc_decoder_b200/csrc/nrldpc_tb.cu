@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(kSegThreads) tb_segment_kernel(const nrldpc_tb
   int local = 0;
   for (int t = t0; t < t1; ++t) {
     TbSeg s;
-    int e = tb_segment(tbs[t].A, tbs[t].G, tbs[t].Qm, tbs[t].bgn, &s);
+    int e = tb_segment(tbs[t].A, tbs[t].G, tbs[t].Qm, tbs[t].bgn, tbs[t].tbs_lbrm, &s);
     if (!e && tbs[t].rv > 3) e = kTbBadArg;
     sp.tb_err[t] = e;
     if (!e) local += s.C;
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kSegThreads) tb_segment_kernel(const nrldpc_tb
     sp.tb_first[t] = cb;
     if (sp.tb_err[t]) continue;
     TbSeg s;
-    tb_segment(tbs[t].A, tbs[t].G, tbs[t].Qm, tbs[t].bgn, &s);
+    tb_segment(tbs[t].A, tbs[t].G, tbs[t].Qm, tbs[t].bgn, tbs[t].tbs_lbrm, &s);
     const int key = tb_graph_key(s.bgn, s.Zc, s.iLS);
     for (int r = 0; r < s.C; ++r, ++cb) {
       const int E = tb_cb_E(s, r);
@@ -114,6 +114,9 @@ __global__ void __launch_bounds__(kSegThreads) tb_segment_kernel(const nrldpc_tb
       c.crctype = s.crc_cb;
       c.llr_off = tbs[t].llr_offset + tb_cb_llr_start(s, r);
       c.bits_off = (int64_t)cb * kCbBitsStride;
+      c.ncb = d.Ncb;
+      c.harq_mode = tbs[t].flags & (NRLDPC_TB_HARQ_COMBINE | NRLDPC_TB_HARQ_STORE);
+      c.harq_off = tbs[t].harq_offset + (int64_t)r * (d.N + 2 * s.Zc);
       sp.cws[cb] = c;
       sp.cb_key[cb] = key;
       atomicAdd(&s_count[key], 1);
@@ -250,7 +253,7 @@ __global__ void __launch_bounds__(128) tb_finish_kernel(const nrldpc_tb_t* __res
     return;
   }
   TbSeg s;
-  tb_segment(tbs[tb].A, tbs[tb].G, tbs[tb].Qm, tbs[tb].bgn, &s);
+  tb_segment(tbs[tb].A, tbs[tb].G, tbs[tb].Qm, tbs[tb].bgn, tbs[tb].tbs_lbrm, &s);
   const int first = fp.tb_first[tb];
   if (tid == 0) {
     s_fail = 0;
@@ -360,11 +363,12 @@ void engine_free(TbEngine* e) {
 }
 
 int engine_decode(TbEngine* e, const nrldpc_tb_t* d_tbs, int n, const int16_t* d_llr, uint8_t* d_out,
-                  int32_t* d_status, int32_t* d_iters, cudaStream_t s) {
+                  int32_t* d_status, int32_t* d_iters, int16_t* d_harq, cudaStream_t s) {
   if (n == 0) return NRLDPC_OK;
   tb_segment_kernel<<<1, kSegThreads, 0, s>>>(d_tbs, n, e->sp);
   count_launch();
   e->mp.llr = d_llr;
+  e->mp.harq = d_harq;
   if (launch_mixed(e->mp, e->grid, e->degen, s) != 0) return NRLDPC_ERR_CUDA;
   FinishParams fp = e->fp;
   fp.out = d_out;
@@ -391,11 +395,12 @@ int32_t nrldpc_tb_segment(const nrldpc_tb_t* tb, nrldpc_tb_info_t* info) {
   if (!tb || !info) return NRLDPC_ERR_ARG;
   memset(info, 0, sizeof(*info));
   TbSeg s;
-  int e = tb_segment(tb->A, tb->G, tb->Qm, tb->bgn, &s);
+  int e = tb_segment(tb->A, tb->G, tb->Qm, tb->bgn, tb->tbs_lbrm, &s);
   if (!e && tb->rv > 3) e = kTbBadArg;
   if (e) {
     static const char* why[] = {"", "bad A, G, Qm, rv or base graph", "does not split into equal byte-aligned code blocks",
-                                "a code block's E exceeds 65535", "a code block gets no coded bits"};
+                                "a code block's E exceeds 65535", "a code block gets no coded bits",
+                                "the limited circular buffer is shorter than the systematic part"};
     fprintf(stderr, "nrldpc_tb_segment: invalid transport block (%s): A=%d G=%d Qm=%d rv=%d bgn=%d\n", why[e], tb->A,
             tb->G, tb->Qm, tb->rv, tb->bgn);
     return NRLDPC_ERR_CONFIG;
@@ -414,6 +419,10 @@ int32_t nrldpc_tb_segment(const nrldpc_tb_t* tb, nrldpc_tb_info_t* info) {
   info->cb_cfg.rv = tb->rv;
   info->cb_cfg.Qm = tb->Qm;
   info->cb_cfg.HARQ_on = 0;
+  const CbDerived d = tb_cb_derive(s, s.E_lo, tb->rv, tb->Qm);
+  info->Ncb = d.Ncb;
+  info->k0 = d.k0;
+  info->harq_elems = (int64_t)s.C * (d.N + 2 * s.Zc);
   return NRLDPC_OK;
 }
 
@@ -548,12 +557,13 @@ int32_t nrldpc_tb_engine_destroy(void* engine) {
 }
 
 int32_t nrldpc_tb_engine_decode(void* engine, const nrldpc_tb_t* d_tbs, int32_t num_tbs, const int16_t* d_llr,
-                                uint8_t* d_out, int32_t* d_status, int32_t* d_iterations, void* stream) {
+                                uint8_t* d_out, int32_t* d_status, int32_t* d_iterations, int16_t* d_harq,
+                                void* stream) {
   TbEngine* e = static_cast<TbEngine*>(engine);
   if (!e || num_tbs < 0 || num_tbs > e->max_tbs) return NRLDPC_ERR_ARG;
   if (num_tbs == 0) return NRLDPC_OK;
   if (!d_tbs || !d_llr || !d_out || !d_status) return NRLDPC_ERR_ARG;
-  return engine_decode(e, d_tbs, num_tbs, d_llr, d_out, d_status, d_iterations,
+  return engine_decode(e, d_tbs, num_tbs, d_llr, d_out, d_status, d_iterations, d_harq,
                        reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -603,7 +613,7 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
   std::vector<int> ncb(n, 0);
   for (int i = 0; i < n && rc == NRLDPC_OK; ++i) {
     TbSeg sg;
-    const int err = tb_segment(tbs[i].A, tbs[i].G, tbs[i].Qm, tbs[i].bgn, &sg);
+    const int err = tb_segment(tbs[i].A, tbs[i].G, tbs[i].Qm, tbs[i].bgn, tbs[i].tbs_lbrm, &sg);
     ncb[i] = (err || tbs[i].rv > 3) ? -1 : sg.C;
     if (ncb[i] > max_cbs) ncb[i] = -1;   // cannot fit any batch: rejected as a configuration error
   }
@@ -690,7 +700,7 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
       const int m = (int)sl.members.size();
       if (cudaMemcpyAsync(sl.d_tbs, sl.h_tbs, (size_t)m * sizeof(nrldpc_tb_t), cudaMemcpyHostToDevice, s) !=
               cudaSuccess ||
-          engine_decode(e, sl.d_tbs, m, d_llr, d_out, sl.d_status, nullptr, s) != NRLDPC_OK ||
+          engine_decode(e, sl.d_tbs, m, d_llr, d_out, sl.d_status, nullptr, nullptr, s) != NRLDPC_OK ||
           cudaMemcpyAsync(sl.h_status, sl.d_status, (size_t)m * sizeof(int32_t), cudaMemcpyDeviceToHost, s) !=
               cudaSuccess ||
           cudaEventRecord(sl.ev, s) != cudaSuccess) {

@@ -25,6 +25,8 @@ struct TbSeg {
   int32_t A_cb;     // code-block information bits (the reference's A field)
   int32_t crc_cb;   // code-block CRC type: 0 CRC16, 1 CRC24A, 2 CRC24B
   int32_t E_lo, E_hi, n_lo;   // code blocks 0..n_lo-1 carry E_lo bits, the rest E_hi
+  int32_t N;        // mother code length after puncturing (66 Zc / 50 Zc)
+  int32_t Ncb;      // circular-buffer length: N, or N_ref with limited-buffer rate matching
 };
 
 // Error codes of tb_segment (0 = valid).
@@ -34,6 +36,7 @@ enum TbSegError : int32_t {
   kTbNotDivisible = 2,   // B + C*L not divisible into equal byte-aligned code blocks (TS 38.214 TBS rule)
   kTbTooLong = 3,        // a code block's E does not fit the 16-bit E field
   kTbTooShort = 4,       // a code block would get no coded bits
+  kTbLbrm = 5,           // the limited circular buffer would cut into the systematic bits
 };
 
 // Smallest lifting size Z = a * 2^j <= 384 (a = 2,3,5,7,9,11,13,15; set index
@@ -54,8 +57,12 @@ __host__ __device__ inline void tb_lifting(int K, int Kb, int* Zc, int* iLS) {
 }
 
 // Code-block segmentation of a transport block of A payload bits coded into G
-// bits with modulation order Qm on base graph bgn (one layer).
-__host__ __device__ inline int32_t tb_segment(int32_t A, int32_t G, int32_t Qm, int32_t bgn, TbSeg* s) {
+// bits with modulation order Qm on base graph bgn (one layer).  tbs_lbrm > 0
+// turns on limited-buffer rate matching (TS 38.212 5.4.2.1): every code block's
+// circular buffer is Ncb = min(N, N_ref), N_ref = floor(TBS_LBRM / (C R_LBRM)),
+// R_LBRM = 2/3.
+__host__ __device__ inline int32_t tb_segment(int32_t A, int32_t G, int32_t Qm, int32_t bgn, int32_t tbs_lbrm,
+                                              TbSeg* s) {
   if (A <= 0 || (A & 7) || (bgn != 1 && bgn != 2) || !(Qm == 1 || Qm == 2 || Qm == 4 || Qm == 6 || Qm == 8) ||
       G <= 0 || G % Qm)
     return kTbBadArg;
@@ -84,6 +91,13 @@ __host__ __device__ inline int32_t tb_segment(int32_t A, int32_t G, int32_t Qm, 
     s->crc_cb = 2;
     if (s->A_cb & 7) return kTbNotDivisible;
   }
+  s->N = (bgn == 1 ? 66 : 50) * s->Zc;
+  s->Ncb = s->N;
+  if (tbs_lbrm > 0) {
+    const int64_t nref = (3 * (int64_t)tbs_lbrm) / (2 * (int64_t)s->C);
+    if (nref < s->N) s->Ncb = (int32_t)nref;
+    if (s->Ncb < ((bgn == 1 ? 22 : 10) - 2) * s->Zc) return kTbLbrm;
+  }
   const int q = G / Qm;   // symbols (one layer)
   s->E_lo = Qm * (q / s->C);
   s->E_hi = Qm * ((q + s->C - 1) / s->C);
@@ -100,9 +114,11 @@ __host__ __device__ inline int64_t tb_cb_llr_start(const TbSeg& s, int r) {
 }
 
 // Derived rate-recovery parameters of one code block (the fields of
-// gen_ldpc_parameters the decode kernels use; Ncb = N, as in the reference).
+// gen_ldpc_parameters the decode kernels use).  With Ncb = N they are the
+// reference's; with a limited buffer k0 = floor(f_rv Ncb / (N_bg Zc)) Zc
+// (TS 38.212 Table 5.4.2.1-2) and only Ncb - F positions take coded bits.
 struct CbDerived {
-  int32_t B, K, N, F, Nv, c0, k0, symbols;
+  int32_t B, K, N, F, Nv, c0, k0, symbols, Ncb;
 };
 __host__ __device__ inline CbDerived tb_cb_derive(const TbSeg& s, int32_t E, int32_t rv, int32_t Qm) {
   CbDerived d;
@@ -112,8 +128,10 @@ __host__ __device__ inline CbDerived tb_cb_derive(const TbSeg& s, int32_t E, int
   d.F = d.K - d.B;
   const int k0_bg1[4] = {0, 17, 33, 56};
   const int k0_bg2[4] = {0, 13, 25, 43};
-  d.k0 = (s.bgn == 1 ? k0_bg1[rv & 3] : k0_bg2[rv & 3]) * s.Zc;
-  d.Nv = d.N - d.F;
+  const int f = s.bgn == 1 ? k0_bg1[rv & 3] : k0_bg2[rv & 3];
+  d.Ncb = s.Ncb;
+  d.k0 = (int32_t)(((int64_t)f * s.Ncb) / ((int64_t)(s.bgn == 1 ? 66 : 50) * s.Zc)) * s.Zc;
+  d.Nv = d.Ncb - d.F;
   const int fill_lo = d.B - 2 * s.Zc, fill_hi = d.K - 2 * s.Zc;
   d.c0 = d.k0 < fill_lo ? d.k0 : (d.k0 < fill_hi ? fill_lo : d.k0 - d.F);
   d.symbols = E / Qm;

@@ -109,9 +109,10 @@ def ldpc_decode(llr: torch.Tensor, inconfig, decoder_config, *, return_app: bool
     return out
 
 
-def ldpc_encode(info: torch.Tensor, inconfig) -> torch.Tensor:
+def ldpc_encode(info: torch.Tensor, inconfig, ncb: int = 0) -> torch.Tensor:
     """Encode a batch of payloads (uint8 CUDA tensor [n, >= A/8], MSB first) into
-    rate-matched bits packed MSB first: uint8 [n, ceil(E/8)]."""
+    rate-matched bits packed MSB first: uint8 [n, ceil(E/8)].  0 < ncb < N selects
+    limited-buffer rate matching over a circular buffer of ncb bits."""
     cfg = _as_in_config(inconfig)
     if not info.is_cuda or info.dtype != torch.uint8 or info.dim() != 2:
         raise ValueError("info must be a uint8 CUDA tensor of shape [n, A/8]")
@@ -124,8 +125,13 @@ def ldpc_encode(info: torch.Tensor, inconfig) -> torch.Tensor:
     lib = capi.load_library()
     stream = torch.cuda.current_stream(info.device).cuda_stream
     with torch.cuda.device(info.device):
-        rc = lib.nrldpc_encode_batch(ctypes.c_void_p(info.data_ptr()), _row_stride(info), n, ctypes.byref(cfg),
-                                     ctypes.c_void_p(out.data_ptr()), _row_stride(out), ctypes.c_void_p(stream))
+        if ncb and 0 < ncb < code_params(cfg).N:
+            rc = lib.nrldpc_encode_batch_ncb(ctypes.c_void_p(info.data_ptr()), _row_stride(info), n,
+                                             ctypes.byref(cfg), int(ncb), ctypes.c_void_p(out.data_ptr()),
+                                             _row_stride(out), ctypes.c_void_p(stream))
+        else:
+            rc = lib.nrldpc_encode_batch(ctypes.c_void_p(info.data_ptr()), _row_stride(info), n, ctypes.byref(cfg),
+                                         ctypes.c_void_p(out.data_ptr()), _row_stride(out), ctypes.c_void_p(stream))
     _check(rc, "nrldpc_encode_batch")
     return out
 

@@ -25,8 +25,11 @@ import numpy as np
 
 from . import capi
 
-TB_DTYPE = np.dtype([("A", "<i4"), ("G", "<i4"), ("Qm", "<u2"), ("rv", "<u2"), ("bgn", "<u2"), ("pad", "<u2"),
-                     ("llr_offset", "<i8"), ("out_offset", "<i8")])
+TB_DTYPE = np.dtype([("A", "<i4"), ("G", "<i4"), ("Qm", "<u2"), ("rv", "<u2"), ("bgn", "<u2"), ("flags", "<u2"),
+                     ("llr_offset", "<i8"), ("out_offset", "<i8"), ("tbs_lbrm", "<i4"), ("pad", "<i4"),
+                     ("harq_offset", "<i8")])
+HARQ_COMBINE = capi.NRLDPC_TB_HARQ_COMBINE   # add this transmission to the stored soft buffers
+HARQ_STORE = capi.NRLDPC_TB_HARQ_STORE       # keep the combined soft buffers for a retransmission
 assert TB_DTYPE.itemsize == ctypes.sizeof(capi.TbDesc)
 
 
@@ -40,6 +43,9 @@ class Segmentation:
     E_hi: int
     n_lo: int
     cb_cfg: Tuple[int, int, int, int, int, int, int]   # (bgn, A_cb, crctype, E_lo, rv, Qm, 0)
+    Ncb: int = 0          # circular-buffer length of every code block
+    k0: int = 0
+    harq_elems: int = 0   # int16 soft-buffer elements of the whole block: C (N + 2Zc)
 
     def E(self, r: int) -> int:
         return self.E_lo if r < self.n_lo else self.E_hi
@@ -48,15 +54,16 @@ class Segmentation:
         return r * self.E_lo if r < self.n_lo else self.n_lo * self.E_lo + (r - self.n_lo) * self.E_hi
 
 
-def segment(A: int, G: int, Qm: int, bgn: int, rv: int = 0) -> Segmentation:
+def segment(A: int, G: int, Qm: int, bgn: int, rv: int = 0, tbs_lbrm: int = 0) -> Segmentation:
+    """TS 38.212 5.2.2 segmentation; tbs_lbrm > 0 adds limited-buffer rate matching."""
     lib = capi.load_library()
-    d = capi.TbDesc(A, G, Qm, rv, bgn, 0, 0, 0)
+    d = capi.TbDesc(A, G, Qm, rv, bgn, 0, 0, 0, int(tbs_lbrm), 0, 0)
     info = capi.TbInfo()
     if lib.nrldpc_tb_segment(ctypes.byref(d), ctypes.byref(info)) != 0:
-        raise ValueError(f"invalid transport block A={A} G={G} Qm={Qm} bgn={bgn} rv={rv}")
+        raise ValueError(f"invalid transport block A={A} G={G} Qm={Qm} bgn={bgn} rv={rv} tbs_lbrm={tbs_lbrm}")
     c = info.cb_cfg
     return Segmentation(info.C, info.L_tb, info.Kp, info.Zc, info.E_lo, info.E_hi, info.n_lo,
-                        (c.bgn, c.A, c.crctype, c.E, c.rv, c.Qm, 0))
+                        (c.bgn, c.A, c.crctype, c.E, c.rv, c.Qm, 0), info.Ncb, info.k0, info.harq_elems)
 
 
 def code_block_count(A: int, bgn: int) -> Tuple[int, int]:
@@ -97,11 +104,16 @@ def round_tbs(A: float, bgn: int) -> int:
         A = A2 if A2 < A else A - 8
 
 
-def tb_array(rows: Sequence[Tuple[int, int, int, int, int, int, int]]) -> np.ndarray:
-    """(A, G, Qm, rv, bgn, llr_offset, out_offset) rows -> nrldpc_tb_t records."""
+def tb_array(rows: Sequence[Tuple[int, ...]]) -> np.ndarray:
+    """(A, G, Qm, rv, bgn, llr_offset, out_offset[, tbs_lbrm[, flags, harq_offset]]) rows
+    -> nrldpc_tb_t records."""
     a = np.zeros(len(rows), dtype=TB_DTYPE)
-    for i, (A, G, Qm, rv, bgn, lo, oo) in enumerate(rows):
-        a[i] = (A, G, Qm, rv, bgn, 0, lo, oo)
+    for i, r in enumerate(rows):
+        A, G, Qm, rv, bgn, lo, oo = r[:7]
+        lbrm = r[7] if len(r) > 7 else 0
+        flags = r[8] if len(r) > 8 else 0
+        ho = r[9] if len(r) > 9 else 0
+        a[i] = (A, G, Qm, rv, bgn, flags, lo, oo, lbrm, 0, ho)
     return a
 
 
@@ -128,9 +140,10 @@ class TbEngine:
         except Exception:
             pass
 
-    def decode(self, tbs: np.ndarray, llr, out, stream=None):
+    def decode(self, tbs: np.ndarray, llr, out, stream=None, harq=None):
         """tbs: nrldpc_tb_t records (numpy); llr: int16 CUDA arena; out: uint8 CUDA
-        arena.  Returns (status, iterations) int32 CUDA tensors."""
+        arena; harq: int16 CUDA soft-buffer arena for blocks with HARQ flags.
+        Returns (status, iterations) int32 CUDA tensors."""
         import torch
 
         dev = llr.device
@@ -142,6 +155,7 @@ class TbEngine:
         rc = self.lib.nrldpc_tb_engine_decode(self.handle, ctypes.c_void_p(d_tbs.data_ptr()), n,
                                               ctypes.c_void_p(llr.data_ptr()), ctypes.c_void_p(out.data_ptr()),
                                               ctypes.c_void_p(status.data_ptr()), ctypes.c_void_p(iters.data_ptr()),
+                                              ctypes.c_void_p(harq.data_ptr() if harq is not None else 0),
                                               ctypes.c_void_p(s.cuda_stream))
         if rc != 0:
             raise RuntimeError(f"nrldpc_tb_engine_decode failed: {rc}")
@@ -212,7 +226,8 @@ def encode_transport_blocks(payloads: List[np.ndarray], tbs: np.ndarray, noise_p
     llr_off, out_off = 0, 0
     segs = []
     for i in range(len(tbs)):
-        sg = segment(int(tbs[i]["A"]), int(tbs[i]["G"]), int(tbs[i]["Qm"]), int(tbs[i]["bgn"]), int(tbs[i]["rv"]))
+        sg = segment(int(tbs[i]["A"]), int(tbs[i]["G"]), int(tbs[i]["Qm"]), int(tbs[i]["bgn"]), int(tbs[i]["rv"]),
+                     int(tbs[i]["tbs_lbrm"]))
         segs.append(sg)
         tbs[i]["llr_offset"] = llr_off
         tbs[i]["out_offset"] = out_off
@@ -235,7 +250,7 @@ def encode_transport_blocks(payloads: List[np.ndarray], tbs: np.ndarray, noise_p
             E = sg.E(lo)
             cfg = (sg.cb_cfg[0], sg.cb_cfg[1], sg.cb_cfg[2], E, sg.cb_cfg[4], sg.cb_cfg[5], 0)
             info = torch.from_numpy(np.stack(chunks[lo:hi])).to(dev)
-            rm = ldpc_encode(info, cfg)
+            rm = ldpc_encode(info, cfg, ncb=sg.Ncb)
             llr = channel_llrs(rm, E, cfg[5], float(noise_power_db[i]), seed=seed * 1000003 + i * 7 + lo)
             start = int(tbs[i]["llr_offset"]) + sg.llr_start(lo)
             arena[start:start + (hi - lo) * E] = llr.reshape(-1)

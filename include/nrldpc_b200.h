@@ -219,6 +219,13 @@ int32_t nrldpc_encode_batch(const uint8_t *d_info, int64_t info_stride,
                             int32_t num_cw, const ldpc_in_config_t *inconfig,
                             uint8_t *d_rm, int64_t rm_stride, void *stream);
 
+/* Same with limited-buffer rate matching (TS 38.212 5.4.2.1): bit selection
+ * over a circular buffer of ncb bits (K - 2Zc <= ncb < N; 0 or >= N: N) with
+ * k0 computed for it.  Returns 0, -1, -2 or -4. */
+int32_t nrldpc_encode_batch_ncb(const uint8_t *d_info, int64_t info_stride,
+                                int32_t num_cw, const ldpc_in_config_t *inconfig, int32_t ncb,
+                                uint8_t *d_rm, int64_t rm_stride, void *stream);
+
 /* Device LLR front-end for num_cw blocks: d_rm uint8 [num_cw][rm_stride]
  * (ceil(E/8) packed bits used) -> d_llr int16 [num_cw][llr_stride] (E
  * values), through the same mapping / AWGN / demapping / quantisation as
@@ -283,16 +290,29 @@ int32_t nrldpc_mixed_plan_destroy(void *plan);
 /* One transport block: A payload bits (multiple of 8), coded into G bits
  * (multiple of Qm, one layer) on base graph bgn.  Its G int16 LLRs start at
  * llr_offset in the LLR arena, code block after code block in order; its A/8
- * decoded payload bytes go to out_offset in the output arena. */
+ * decoded payload bytes go to out_offset in the output arena.
+ * tbs_lbrm > 0 selects limited-buffer rate matching (TS 38.212 5.4.2.1): each
+ * code block's circular buffer holds Ncb = min(N, floor(3 tbs_lbrm / (2 C)))
+ * bits (the reference always uses Ncb = N).
+ * HARQ: with a soft-buffer arena passed to the decode call, code block r of
+ * this block keeps its soft buffer (N + 2 Zc int16) at harq_offset +
+ * r (N + 2 Zc); flags NRLDPC_TB_HARQ_COMBINE adds the received LLRs to the
+ * stored soft buffer (retransmission with any rv), NRLDPC_TB_HARQ_STORE writes
+ * the combined soft buffer back. */
+#define NRLDPC_TB_HARQ_COMBINE 1
+#define NRLDPC_TB_HARQ_STORE 2
 typedef struct {
     int32_t A;
     int32_t G;
     uint16_t Qm;
     uint16_t rv;
     uint16_t bgn;
-    uint16_t pad;
+    uint16_t flags;
     int64_t llr_offset;
     int64_t out_offset;
+    int32_t tbs_lbrm;
+    int32_t pad;
+    int64_t harq_offset;
 } nrldpc_tb_t;
 
 /* Segmentation of one transport block (host). */
@@ -304,6 +324,9 @@ typedef struct {
     int32_t E_lo, E_hi; /* code blocks 0..n_lo-1 carry E_lo coded bits, the rest E_hi */
     int32_t n_lo;
     ldpc_in_config_t cb_cfg;   /* per-code-block decoder configuration (E = E_lo) */
+    int32_t Ncb;        /* circular-buffer length of every code block */
+    int32_t k0;         /* start position of the block's rv in the circular buffer */
+    int64_t harq_elems; /* int16 soft-buffer elements of the whole block: C (N + 2 Zc) */
 } nrldpc_tb_info_t;
 
 /* Returns 0, or NRLDPC_ERR_CONFIG with a reason on stderr: bad A / G / Qm /
@@ -328,9 +351,12 @@ int32_t nrldpc_tb_engine_destroy(void *engine);
  * are in d_llr.  Writes the payload bytes of every block to d_out, d_status
  * [num_tbs] (0 CRC pass, 1 fail, -2 bad configuration, -4 batch over the
  * engine's capacity) and d_iterations [num_tbs] (largest code-block iteration
- * count; nullable).  Stream-ordered, no host synchronisation. */
+ * count; nullable).  d_harq (nullable) is the int16 soft-buffer arena the
+ * blocks' HARQ flags and offsets refer to.  Stream-ordered, no host
+ * synchronisation. */
 int32_t nrldpc_tb_engine_decode(void *engine, const nrldpc_tb_t *d_tbs, int32_t num_tbs, const int16_t *d_llr,
-                                uint8_t *d_out, int32_t *d_status, int32_t *d_iterations, void *stream);
+                                uint8_t *d_out, int32_t *d_status, int32_t *d_iterations, int16_t *d_harq,
+                                void *stream);
 
 /* Device views of the last batch's code blocks, for inspection: hard bits
  * [max_cbs][1056] bytes, status and iterations [max_cbs], and each transport

@@ -124,10 +124,25 @@ int orc_derive(const orc_in_config_t *in, orc_params_t *p) {
     p->F = p->K - p->B;
     static const int k0a[4] = {0, 17, 33, 56}, k0b[4] = {0, 13, 25, 43};
     p->k0 = (in->bgn == 1 ? k0a : k0b)[in->rv] * p->Zc;
+    p->Ncb = p->N;
     const graph_t *g = graph(in->bgn);
     p->rows = g->rows;
     p->cols = g->cols;
     p->nnz = g->nnz;
+    return 0;
+}
+
+int orc_set_ncb(orc_params_t *p, int ncb) {
+    if (ncb <= 0 || ncb >= p->N) {
+        p->Ncb = p->N;
+        return 0;
+    }
+    if (ncb < p->K - 2 * p->Zc) return -1;
+    static const int fa[4] = {0, 17, 33, 56}, fb[4] = {0, 13, 25, 43};
+    const int f = (p->bgn == 1 ? fa : fb)[p->rv];
+    const int nbg = p->bgn == 1 ? 66 : 50;
+    p->Ncb = ncb;
+    p->k0 = (int)(((long long)f * ncb) / ((long long)nbg * p->Zc)) * p->Zc;
     return 0;
 }
 
@@ -168,7 +183,7 @@ void orc_rate_recover(const orc_params_t *p, int16_t fill, const int16_t *llr, i
             harq[pos + 2 * Zc] = (int16_t)(harq[pos + 2 * Zc] + llr[idx]);
             k++;
         }
-        pos = (pos + 1) % N;
+        pos = (pos + 1) % p->Ncb;
     }
 }
 
@@ -497,17 +512,18 @@ int32_t orc_encode_codeword(const uint8_t *infobytes, uint8_t *cw_bits, const or
 
 /* c_lib/ldpc_rate_match.c:27-106: bit selection from k0 over the circular
  * buffer without filler bits, then the Qm row/column interleave. */
-int32_t orc_encode(const uint8_t *infobytes, uint8_t *rm_bytes, const orc_in_config_t *in) {
-    orc_params_t p;
-    if (orc_derive(in, &p) != 0) return -2;
+int32_t orc_encode_params(const uint8_t *infobytes, uint8_t *rm_bytes, const orc_params_t *pp) {
+    const orc_params_t p = *pp;
     static uint8_t cw[BG1_COLS * MAX_ZC];
     static uint8_t e[65536];
-    orc_encode_codeword(infobytes, cw, in);
-    const int Zc = p.Zc, N = p.N;
+    orc_in_config_t in = {(uint16_t)p.bgn, (uint16_t)p.A, (uint16_t)p.crctype, (uint16_t)p.E,
+                          (uint16_t)p.rv, (uint16_t)p.Qm, 0};
+    orc_encode_codeword(infobytes, cw, &in);
+    const int Zc = p.Zc;
     int k = 0, pos = p.k0;
     while (k < p.E) {
         if (pos < p.B - 2 * Zc || pos >= p.K - 2 * Zc) e[k++] = cw[pos + 2 * Zc];
-        pos = (pos + 1) % N;
+        pos = (pos + 1) % p.Ncb;
     }
     const int sym = p.E / p.Qm;
     memset(rm_bytes, 0, (size_t)(p.E + 7) / 8);
@@ -516,6 +532,12 @@ int32_t orc_encode(const uint8_t *infobytes, uint8_t *rm_bytes, const orc_in_con
         if (e[b * sym + s]) rm_bytes[t / 8] |= (uint8_t)(0x80 >> (t % 8));
     }
     return 0;
+}
+
+int32_t orc_encode(const uint8_t *infobytes, uint8_t *rm_bytes, const orc_in_config_t *in) {
+    orc_params_t p;
+    if (orc_derive(in, &p) != 0) return -2;
+    return orc_encode_params(infobytes, rm_bytes, &p);
 }
 
 /* -------------------------------------------------------------- channel */

@@ -34,6 +34,7 @@ typedef struct {
     int bgn, A, crctype, E, rv, Qm, HARQ_on;
     int B, Zc, iLS, K, F, N, k0;
     int rows, cols, nnz;
+    int Ncb;   /* circular-buffer length: N, or less with limited-buffer rate matching */
 } orc_params_t;
 
 /* gen_ldpc_parameters (c_lib/ldpc_internal.c:66-170). 0 ok, -1 invalid. */
@@ -44,6 +45,15 @@ int orc_derive(const orc_in_config_t *in, orc_params_t *p);
  * col[nnz] base columns, shift[nnz] = Vij mod Zc for the configuration's
  * lifting set, off[rows+1] row offsets.  Returns nnz, or -1. */
 int orc_graph(const orc_params_t *p, int32_t *col, int32_t *shift, int32_t *off);
+
+/* Limited-buffer rate matching (TS 38.212 5.4.2.1): circular buffer of ncb
+ * bits (0 < ncb < N; ncb >= K-2Zc so the systematic part is whole) and k0
+ * recomputed for it.  The reference always uses Ncb = N; this is restated from
+ * the standard as py5gphy/ldpc/nr_ldpc_ratematch.py:48-67 does.  0 ok, -1 bad. */
+int orc_set_ncb(orc_params_t *p, int ncb);
+
+/* Rate matching of one block with explicit parameters (Ncb honoured). */
+int32_t orc_encode_params(const uint8_t *infobytes, uint8_t *rm_bytes, const orc_params_t *p);
 
 /* calculate_crc (c_lib/nr_crc.c:170-179). */
 uint32_t orc_crc(const uint8_t *data, int len, int crctype);

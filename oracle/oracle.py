@@ -42,7 +42,7 @@ class DecCfg(ctypes.Structure):
 class OrcParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (
         "bgn", "A", "crctype", "E", "rv", "Qm", "HARQ_on", "B", "Zc", "iLS", "K", "F", "N", "k0",
-        "rows", "cols", "nnz")]
+        "rows", "cols", "nnz", "Ncb")]
 
 
 class RefConfig(ctypes.Structure):
@@ -100,6 +100,13 @@ class Oracle:
         L.orc_channel.restype = ctypes.c_int
         L.orc_set_trained.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.orc_set_degree_alpha.argtypes = [ctypes.c_void_p]
+        L.orc_set_ncb.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_int]
+        L.orc_set_ncb.restype = ctypes.c_int
+        L.orc_encode_params.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(OrcParams)]
+        L.orc_encode_params.restype = ctypes.c_int32
+        L.orc_decode_recovered.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(OrcParams),
+                                           ctypes.POINTER(DecCfg), ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_decode_recovered.restype = ctypes.c_int32
         L.orc_graph.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.orc_graph.restype = ctypes.c_int
         self.harq = np.zeros(68 * 384, dtype=np.int16)
@@ -108,6 +115,40 @@ class Oracle:
         p = OrcParams()
         rc = self.lib.orc_derive(ctypes.byref(cfg), ctypes.byref(p))
         return rc, p
+
+    def params(self, cfg: InConfig, ncb: int = 0) -> OrcParams:
+        """Derived parameters, with limited-buffer rate matching when 0 < ncb < N."""
+        rc, p = self.derive(cfg)
+        if rc != 0 or self.lib.orc_set_ncb(ctypes.byref(p), int(ncb)) != 0:
+            raise ValueError("invalid configuration")
+        return p
+
+    def encode_ncb(self, payload: np.ndarray, cfg: InConfig, ncb: int) -> np.ndarray:
+        p = self.params(cfg, ncb)
+        payload = np.ascontiguousarray(payload, dtype=np.uint8)
+        out = np.zeros((cfg.E + 7) // 8 + 8, dtype=np.uint8)
+        assert self.lib.orc_encode_params(_p(payload), _p(out), ctypes.byref(p)) == 0
+        return out[: (cfg.E + 7) // 8].copy()
+
+    def rate_recover_ncb(self, cfg: InConfig, ncb: int, fill: int, llr: np.ndarray, harq: np.ndarray | None = None):
+        """Soft buffer after rate recovery with circular-buffer length ncb; with
+        cfg.HARQ_on the LLRs are added to `harq` (int16 wrap-around, in place)."""
+        p = self.params(cfg, ncb)
+        h = np.zeros(68 * 384, dtype=np.int16) if harq is None else harq
+        llr = np.ascontiguousarray(llr, dtype=np.int16)
+        self.lib.orc_rate_recover(ctypes.byref(p), fill, _p(llr), _p(h))
+        return h
+
+    def decode_soft(self, harq: np.ndarray, cfg: InConfig, dcfg: DecCfg):
+        """Decode a recovered soft buffer: (status, bits, iterations, final LQ)."""
+        rc, p = self.derive(cfg)
+        bits = np.zeros((p.B + 7) // 8, dtype=np.uint8)
+        lq = np.zeros(p.N + 2 * p.Zc, dtype=np.float32 if dcfg.algo in (0, 4) else np.int16)
+        it = ctypes.c_int32(0)
+        h = np.ascontiguousarray(harq, dtype=np.int16)
+        st = self.lib.orc_decode_recovered(_p(h), _p(bits), ctypes.byref(p), ctypes.byref(dcfg), _p(lq),
+                                           ctypes.byref(it))
+        return int(st), bits, int(it.value), lq
 
     def graph(self, cfg: InConfig):
         """(params, col[nnz], shift[nnz] = Vij mod Zc, off[rows+1]) of one configuration."""

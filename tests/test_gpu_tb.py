@@ -179,3 +179,98 @@ def test_serving_admission_drops_over_budget(cuda):
     assert dropped.sum() == len(tbs) - 3 and res.stats["dropped"] == len(tbs) - 3
     assert np.all(res.status[~dropped] == 0)
     assert np.all(np.isnan(res.latency_s[dropped])) and np.all(np.isfinite(res.latency_s[~dropped]))
+
+
+def test_limited_buffer_encoder_matches_oracle(cuda, oracle):
+    """Device rate matching over a limited circular buffer equals the oracle's
+    (itself pinned to py5gphy), every rv."""
+    from oracle.oracle import in_config
+
+    from deeplearning_5g_ldpc_decoder_b200.decoder import ldpc_encode
+
+    rng = np.random.default_rng(31)
+    for bgn, A, crc, E, Qm, ncb in [(1, 8424, 2, 12000, 8, 18000), (1, 3816, 2, 9000, 4, 10000),
+                                    (2, 3816, 2, 8000, 4, 9000), (2, 1000, 1, 2400, 2, 2600)]:
+        for rv in range(4):
+            cfg = (bgn, A, crc, E, rv, Qm, 0)
+            pay = rng.integers(0, 256, (3, A // 8), dtype=np.uint8)
+            rm = ldpc_encode(torch.from_numpy(pay).to(cuda), cfg, ncb=ncb).cpu().numpy()
+            for i in range(3):
+                assert np.array_equal(rm[i], oracle.encode_ncb(pay[i], in_config(*cfg), ncb)), (cfg, ncb, i)
+
+
+def _harq_expect(oracle, t, arena_h, soft):
+    """Oracle soft buffers (combined into `soft`, a list per code block) and per
+    code block decode results for one transmission of transport block t."""
+    from oracle import tb_ref  # noqa: F401
+    from oracle.oracle import dec_cfg, in_config
+
+    from deeplearning_5g_ldpc_decoder_b200 import tb
+
+    sg = tb.segment(int(t["A"]), int(t["G"]), int(t["Qm"]), int(t["bgn"]), int(t["rv"]), int(t["tbs_lbrm"]))
+    res = []
+    for r in range(sg.C):
+        E = sg.E(r)
+        cfg = (sg.cb_cfg[0], sg.cb_cfg[1], sg.cb_cfg[2], E, sg.cb_cfg[4], sg.cb_cfg[5],
+               1 if (int(t["flags"]) & tb.HARQ_COMBINE) else 0)
+        lo = int(t["llr_offset"]) + sg.llr_start(r)
+        oracle.rate_recover_ncb(in_config(*cfg), sg.Ncb, 1280, arena_h[lo:lo + E], soft[r])
+        res.append(oracle.decode_soft(soft[r], in_config(*cfg[:6], 0), dec_cfg(ROW)))
+    return sg, res
+
+
+def test_harq_retransmission_with_limited_buffer(cuda, oracle):
+    """rv 0 then rv 2 of the same blocks with limited-buffer rate matching: the
+    device soft buffers after each transmission equal the oracle's HARQ
+    combining, every code block decodes as the oracle does from them, and more
+    blocks pass after the retransmission."""
+    from deeplearning_5g_ldpc_decoder_b200 import tb
+    from deeplearning_5g_ldpc_decoder_b200.tb import TbEngine
+
+    rng = np.random.default_rng(44)
+    specs = [(60000, 0.75, 4, 8.3), (20000, 0.8, 6, 14.0), (3000, 0.7, 2, 2.5), (100000, 0.7, 8, 18.5)]
+    rows, pays = [], []
+    harq_off = 0
+    segs = []
+    for A0, R, Qm, snr in specs:
+        bgn = tb.select_bg(int(A0), R)
+        A = tb.round_tbs(A0, bgn)
+        G = tb.coded_bits(A, bgn, Qm, R)
+        lbrm = int(A * 1.2)
+        sg = tb.segment(A, G, Qm, bgn, 0, tbs_lbrm=lbrm)
+        rows.append([A, G, Qm, 0, bgn, 0, 0, lbrm, tb.HARQ_STORE, harq_off])
+        harq_off += sg.harq_elems
+        pays.append(rng.integers(0, 256, A // 8, dtype=np.uint8))
+        segs.append(sg)
+    noise = [-s[3] for s in specs]
+    harq = torch.zeros(harq_off, dtype=torch.int16, device=cuda)
+    soft = [[np.zeros(68 * 384, dtype=np.int16) for _ in range(sg.C)] for sg in segs]
+    eng = TbEngine(max_tbs=16, max_cbs=256, decoder_row=ROW)
+    passed = []
+    for tx, rv in enumerate((0, 2)):
+        for r in rows:
+            r[3] = rv
+            r[8] = tb.HARQ_STORE | (tb.HARQ_COMBINE if tx else 0)
+        tbs, arena, out_bytes = tb.encode_transport_blocks(pays, tb.tb_array([tuple(r) for r in rows]), noise,
+                                                           seed=70 + tx, device=cuda)
+        out = torch.zeros(out_bytes + 8, dtype=torch.uint8, device=cuda)
+        st, _ = eng.decode(tbs, arena, out, harq=harq)
+        torch.cuda.synchronize()
+        st = st.cpu().numpy()
+        arena_h, harq_h = arena.cpu().numpy(), harq.cpu().numpy()
+        p_bits, p_st, p_it, p_first = eng.views()
+        first = _dev_array(p_first, len(tbs), torch.int32, cuda)
+        for i, t in enumerate(tbs):
+            sg, res = _harq_expect(oracle, t, arena_h, soft[i])
+            L = 52 * sg.Zc if int(t["bgn"]) == 2 else 68 * sg.Zc
+            cb_st = _dev_array(p_st + 4 * int(first[i]), sg.C, torch.int32, cuda)
+            cb_it = _dev_array(p_it + 4 * int(first[i]), sg.C, torch.int32, cuda)
+            for r in range(sg.C):
+                base = int(t["harq_offset"]) + r * L
+                assert np.array_equal(harq_h[base:base + L], soft[i][r][:L]), (tx, i, r)
+                assert (cb_st[r], cb_it[r]) == (res[r][0], res[r][2]), (tx, i, r)
+            if st[i] == 0:
+                o = int(t["out_offset"])
+                assert np.array_equal(out.cpu().numpy()[o:o + int(t["A"]) // 8], pays[i])
+        passed.append(int((st == 0).sum()))
+    assert passed[1] > passed[0]

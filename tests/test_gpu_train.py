@@ -223,7 +223,7 @@ def test_float64_kernels_agree_with_float32_path(cuda):
     m64 = _model(cfg, 4, "checkpoint", seed=5).double()
     _, f64 = m64(llr.double(), return_llr=True)
     assert f64.dtype == torch.float64
-    err = (f64 - f32.double()).abs().max() / f64.abs().max()
+    err = ((f64 - f32.double()).abs().max() / f64.abs().max()).detach()
     assert float(err) < 1e-4
 
 

@@ -108,3 +108,51 @@ def test_segmentation_rejects_bad_blocks():
         tb.segment(99992, 300000, 2, 1)       # does not split into equal byte-aligned code blocks
     with pytest.raises(ValueError):
         tb.segment(1000, 3000, 3, 1)          # bad Qm
+
+
+LBRM_GOLDEN = os.path.join(REPO, "tests", "golden", "lbrm_vectors.npz")
+
+
+def test_limited_buffer_oracle_matches_py5gphy(oracle):
+    """The oracle's limited-buffer rate matching and recovery reproduce py5gphy's
+    (k0, selected bits, recovered soft values outside the filler positions)."""
+    from oracle.oracle import in_config
+
+    g = np.load(LBRM_GOLDEN)
+    for i, (bgn, A, crc, E, rv, Qm, ncb) in enumerate(g["cases"]):
+        cfg = in_config(*[int(x) for x in (bgn, A, crc, E, rv, Qm)])
+        p = oracle.params(cfg, int(ncb))
+        assert p.k0 == int(g[f"k0_{i}"][0]) and p.Ncb == int(ncb)
+        rm = np.unpackbits(oracle.encode_ncb(g[f"pay_{i}"], cfg, int(ncb)))[: int(E)]
+        assert np.array_equal(rm, g[f"rm_{i}"]), i
+        h = oracle.rate_recover_ncb(cfg, int(ncb), 1280, g[f"llr_{i}"])[: p.N + 2 * p.Zc]
+        keep = np.ones(p.N, dtype=bool)
+        keep[p.B - 2 * p.Zc: p.K - 2 * p.Zc] = False
+        assert np.array_equal(h[2 * p.Zc:][keep].astype(np.float64), g[f"rec_{i}"][keep]), i
+
+
+def test_library_limited_buffer_segmentation(oracle):
+    """Ncb = min(N, floor(3 TBS_LBRM / 2C)) per code block and k0 from it agree
+    with the oracle's TS 38.212 restatement; a buffer that would cut into the
+    systematic bits is rejected."""
+    from oracle.oracle import in_config
+
+    from deeplearning_5g_ldpc_decoder_b200 import tb
+
+    rng = np.random.default_rng(17)
+    checked = 0
+    for A, G, Qm, rv, bgn in _random_tbs(rng, 300):
+        C, _ = tb.code_block_count(A, bgn)
+        lbrm = int(rng.integers(A // 2, 3 * A))
+        try:
+            sg = tb.segment(A, G, Qm, bgn, rv, tbs_lbrm=lbrm)
+        except ValueError:
+            full = tb.segment(A, G, Qm, bgn, rv)
+            K = (22 if bgn == 1 else 10) * full.Zc
+            assert (3 * lbrm) // (2 * C) < K - 2 * full.Zc
+            continue
+        p = oracle.params(in_config(*sg.cb_cfg[:6]), min((3 * lbrm) // (2 * C), 10 ** 9))
+        assert sg.Ncb == p.Ncb and sg.k0 == p.k0, (A, G, Qm, rv, bgn, lbrm)
+        assert sg.harq_elems == C * (p.N + 2 * p.Zc)
+        checked += 1
+    assert checked > 150
