@@ -672,11 +672,13 @@ int32_t nrldpc_decode_batch_host(const int16_t* h_llr, int64_t llr_stride, int32
   if (make_plan(cp, *decoder_cfg, num_cw, st, &probe) != 0) return NRLDPC_ERR_CUDA;
   const bool fixed = decoder_cfg->algo >= 1 && decoder_cfg->algo <= 3;
   const int64_t wave_cw = (int64_t)(fixed ? 2 : 1) * probe.p.G * probe.grid;
+  // One wave per chunk (at most 32 chunks): the copy of the first chunk is the
+  // only one not hidden behind a decode.
   int64_t chunk = num_cw;
-  constexpr int kChunks = 5;
+  constexpr int kMaxChunks = 32;
   if (wave_cw > 0 && num_cw >= 3 * wave_cw) {
-    const int64_t want = (num_cw + kChunks - 1) / kChunks;
-    chunk = (want + wave_cw - 1) / wave_cw * wave_cw;
+    const int64_t want = (num_cw + kMaxChunks - 1) / kMaxChunks;
+    chunk = std::max<int64_t>(wave_cw, (want + wave_cw - 1) / wave_cw * wave_cw);
   }
   const int nchunks = (int)((num_cw + chunk - 1) / chunk);
   while ((int)hs.h2d.size() < nchunks) {
