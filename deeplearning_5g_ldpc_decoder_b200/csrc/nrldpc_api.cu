@@ -488,6 +488,32 @@ int make_train_params(const ldpc_in_config_t* cfg, int32_t T, int32_t batch, dou
   return NRLDPC_OK;
 }
 
+// Code blocks per CTA (G) that put the most code blocks on an SM, given the
+// kernel's registers and shared memory (one or two (N+2Zc)-value arrays per
+// block); the largest G among equals.  Returns the blocks per SM of that
+// choice and sets p->G, *block, *smem.
+int pick_train_groups(TrainParams* p, bool backward, bool f64, int* block, int* smem) {
+  const int per = (backward ? 2 : 1) * p->n * (f64 ? 8 : 4);
+  const int smem_cap = 227 * 1024 - 1024;
+  const int gmax = std::max(1, kThreadsTarget / p->Zc);
+  int best_g = 0, best_cw = 0, best_occ = 0;
+  for (int G = gmax; G >= 1; --G) {
+    if (G * per > smem_cap) continue;
+    const int blk = (G * p->Zc + 31) & ~31;
+    const int occ = occupancy_train(backward, f64, p->R == 42, blk, G * per);
+    if (occ * G > best_cw) {
+      best_cw = occ * G;
+      best_g = G;
+      best_occ = occ;
+    }
+  }
+  if (best_g == 0) return 0;
+  p->G = best_g;
+  *block = (best_g * p->Zc + 31) & ~31;
+  *smem = best_g * per;
+  return best_occ;
+}
+
 int train_forward(const void* d_llr, int32_t batch, const ldpc_in_config_t* cfg, int32_t iterations,
                   const void* d_alpha, const void* d_beta, double clip, void* d_final, void* d_iter, void* d_ck_lq,
                   uint32_t* d_ck_lr, void* stream, bool f64) {
@@ -507,7 +533,7 @@ int train_forward(const void* d_llr, int32_t batch, const ldpc_in_config_t* cfg,
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int occ = std::max(1, occupancy_train(false, f64, block, smem_f));
+  const int occ = std::max(1, pick_train_groups(&p, false, f64, &block, &smem_f));
   const int items = (batch + p.G - 1) / p.G;
   const int grid = std::max(1, std::min(items, occ * sms));
   return launch_train_forward(p, f64, grid, block, smem_f, stream) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
@@ -538,7 +564,7 @@ int train_backward(const void* d_llr, int32_t batch, const ldpc_in_config_t* cfg
   std::lock_guard<std::mutex> lock(g_mu);
   DeviceState* st = nullptr;
   if (device_state(&st) != 0) return NRLDPC_ERR_CUDA;
-  const int occ = std::max(1, occupancy_train(true, f64, block, smem_b));
+  const int occ = std::max(1, pick_train_groups(&p, true, f64, &block, &smem_b));
   const int items = (batch + p.G - 1) / p.G;
   const int grid = std::max(1, std::min(items, occ * st->num_sms));
   p.scratch_per_cta = (int64_t)p.G * p.nnz * p.Zc;

@@ -183,7 +183,7 @@ struct TrainParams {
 int launch_encode(const EncodeParams& p, void* stream);
 int launch_train_forward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream);
 int launch_train_backward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream);
-int occupancy_train(bool backward, bool f64, int block, int smem);
+int occupancy_train(bool backward, bool f64, bool bg2, int block, int smem);
 int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream);
 int prepare_mixed(bool degen_clip);
 int occupancy_mixed(bool degen_clip);

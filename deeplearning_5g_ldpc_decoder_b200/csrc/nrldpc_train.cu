@@ -221,10 +221,12 @@ __device__ __forceinline__ void train_row_bwd(const TrainParams& p, Real* __rest
     case 8: FN<8, R>(__VA_ARGS__); break;        \
     case 9: FN<9, R>(__VA_ARGS__); break;        \
     case 10: FN<10, R>(__VA_ARGS__); break;      \
-    default: FN<19, R>(__VA_ARGS__); break;      \
+    default: FN<(kMaxD > 10 ? 19 : 10), R>(__VA_ARGS__); break;      \
   }
 
-template <typename Real>
+// kMaxD: the largest row degree of the base graph (19 for BG1, 10 for BG2); a
+// BG2 instantiation carries no degree-19 code and needs half the registers.
+template <typename Real, int kMaxD>
 __global__ void __launch_bounds__(kThreadsTarget) train_forward_kernel(const __grid_constant__ TrainParams p) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   Real* s_lq = reinterpret_cast<Real*>(s_raw);
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(kThreadsTarget) train_forward_kernel(const __g
   }
 }
 
-template <typename Real>
+template <typename Real, int kMaxD>
 __global__ void __launch_bounds__(kThreadsTarget) train_backward_kernel(const __grid_constant__ TrainParams p) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   __shared__ Real s_red[2][2][kThreadsTarget / 32];   // [row parity][alpha, beta][warp]
@@ -381,22 +383,38 @@ int occupancy_one(K kernel, int block, int smem) {
 
 }  // namespace
 
+// BG2 has 42 rows and degrees up to 10; BG1 46 rows and one row of degree 19.
 int launch_train_forward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream) {
-  return f64 ? launch_one(train_forward_kernel<double>, p, grid, block, smem, stream)
-             : launch_one(train_forward_kernel<float>, p, grid, block, smem, stream);
+  const bool bg2 = p.R == 42;
+  if (f64)
+    return bg2 ? launch_one(train_forward_kernel<double, 10>, p, grid, block, smem, stream)
+               : launch_one(train_forward_kernel<double, 19>, p, grid, block, smem, stream);
+  return bg2 ? launch_one(train_forward_kernel<float, 10>, p, grid, block, smem, stream)
+             : launch_one(train_forward_kernel<float, 19>, p, grid, block, smem, stream);
 }
 
 int launch_train_backward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream) {
-  return f64 ? launch_one(train_backward_kernel<double>, p, grid, block, smem, stream)
-             : launch_one(train_backward_kernel<float>, p, grid, block, smem, stream);
+  const bool bg2 = p.R == 42;
+  if (f64)
+    return bg2 ? launch_one(train_backward_kernel<double, 10>, p, grid, block, smem, stream)
+               : launch_one(train_backward_kernel<double, 19>, p, grid, block, smem, stream);
+  return bg2 ? launch_one(train_backward_kernel<float, 10>, p, grid, block, smem, stream)
+             : launch_one(train_backward_kernel<float, 19>, p, grid, block, smem, stream);
 }
 
-int occupancy_train(bool backward, bool f64, int block, int smem) {
-  if (backward)
-    return f64 ? occupancy_one(train_backward_kernel<double>, block, smem)
-               : occupancy_one(train_backward_kernel<float>, block, smem);
-  return f64 ? occupancy_one(train_forward_kernel<double>, block, smem)
-             : occupancy_one(train_forward_kernel<float>, block, smem);
+int occupancy_train(bool backward, bool f64, bool bg2, int block, int smem) {
+  if (backward) {
+    if (f64)
+      return bg2 ? occupancy_one(train_backward_kernel<double, 10>, block, smem)
+                 : occupancy_one(train_backward_kernel<double, 19>, block, smem);
+    return bg2 ? occupancy_one(train_backward_kernel<float, 10>, block, smem)
+               : occupancy_one(train_backward_kernel<float, 19>, block, smem);
+  }
+  if (f64)
+    return bg2 ? occupancy_one(train_forward_kernel<double, 10>, block, smem)
+               : occupancy_one(train_forward_kernel<double, 19>, block, smem);
+  return bg2 ? occupancy_one(train_forward_kernel<float, 10>, block, smem)
+             : occupancy_one(train_forward_kernel<float, 19>, block, smem);
 }
 
 }  // namespace nrldpc
