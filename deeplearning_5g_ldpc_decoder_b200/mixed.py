@@ -124,11 +124,11 @@ class MixedPlan:
 
 
 def random_mixed_configs(n: int, seed: int = 0, bg1_share: float = 0.6, rate=(0.2, 0.92), qms=(2, 4, 6, 8),
-                         lib=None):
+                         lib=None, rvs=(0, 1, 2, 3)):
     """Configurations of the mixed-size workload: lifting size uniform over the
     51 sizes (redrawn where a base graph cannot reach it), BG1 with probability
-    bg1_share, code rate uniform in `rate`, Qm from `qms`, rv and CRC24 type
-    random.  Returns a list of (bgn, A, crctype, E, rv, Qm)."""
+    bg1_share, code rate uniform in `rate`, Qm from `qms`, rv from `rvs` and CRC24
+    type random.  Returns a list of (bgn, A, crctype, E, rv, Qm)."""
     import numpy as np
 
     lib = lib or capi.load_library()
@@ -154,5 +154,5 @@ def random_mixed_configs(n: int, seed: int = 0, bg1_share: float = 0.6, rate=(0.
         E = int(round(B / R / Qm)) * Qm
         if E < Qm or E > 65535:
             continue
-        out.append((bgn, A, crc, E, int(rng.integers(4)), Qm))
+        out.append((bgn, A, crc, E, int(rvs[rng.integers(len(rvs))]), Qm))
     return out
