@@ -11,7 +11,7 @@
 //     work items for the mixed kernel (largest lifting sizes first);
 //  2. fixed_mixed_kernel (nrldpc_mixed.cu), reading its item count from the
 //     device;
-//  3. tb_finish_kernel (one CTA per transport block): code-block verdicts,
+//  3. tb_finish_kernel (one 512-thread CTA per transport block): code-block verdicts,
 //     transport-block CRC as the XOR of per-code-block remainders shifted by
 //     x^(bits after the block) mod g(x), and the payload bytes gathered.
 #include <cuda_runtime.h>
@@ -231,7 +231,7 @@ struct FinishParams {
   int32_t* iters;
 };
 
-__global__ void __launch_bounds__(128) tb_finish_kernel(const nrldpc_tb_t* __restrict__ tbs, int n,
+__global__ void __launch_bounds__(512) tb_finish_kernel(const nrldpc_tb_t* __restrict__ tbs, int n,
                                                         const __grid_constant__ FinishParams fp) {
   const int tb = blockIdx.x;
   if (tb >= n) return;
@@ -374,7 +374,7 @@ int engine_decode(TbEngine* e, const nrldpc_tb_t* d_tbs, int n, const int16_t* d
   fp.out = d_out;
   fp.status = d_status;
   fp.iters = d_iters;
-  tb_finish_kernel<<<n, 128, 0, s>>>(d_tbs, n, fp);
+  tb_finish_kernel<<<n, 512, 0, s>>>(d_tbs, n, fp);
   count_launch();
   return cudaGetLastError() == cudaSuccess ? NRLDPC_OK : NRLDPC_ERR_CUDA;
 }
