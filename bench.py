@@ -171,7 +171,7 @@ def cpu_baseline(per_proc: int = 0, procs: int = 0) -> dict:
 
     kind = "reference" if os.path.exists(REF_SO) else "port"
     procs = procs or len(os.sched_getaffinity(0)) or 1
-    per_proc = per_proc or 96
+    per_proc = per_proc or 768   # about 10 s of decoding per process on the B200 hosts
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
