@@ -297,12 +297,9 @@ __global__ void __launch_bounds__(512) tb_finish_kernel(const nrldpc_tb_t* __res
   }
 }
 
-struct TbEngine {
-  int device = 0, num_sms = 0;
-  int max_tbs = 0, max_cbs = 0, max_items = 0, max_slots = 0;
-  bool degen = false;
-  int grid = 1;
-  MixedGraph* d_graphs = nullptr;
+// Buffers and launch parameters of one batch in flight.  The engine has one
+// lane per batch that may run concurrently (the serving loop's pipeline depth).
+struct TbLane {
   MixedCw* d_cws = nullptr;
   int32_t* d_cb_key = nullptr;
   int32_t* d_tb_first = nullptr;
@@ -315,10 +312,21 @@ struct TbEngine {
   int32_t* d_cb_status = nullptr;
   int32_t* d_cb_iters = nullptr;
   uint32_t* d_scratch = nullptr;
-  const uint32_t* d_crc_tab = nullptr;
   SegParams sp = {};
   MixedParams mp = {};
   FinishParams fp = {};
+};
+
+struct TbEngine {
+  int device = 0, num_sms = 0;
+  int max_tbs = 0, max_cbs = 0, max_items = 0, max_slots = 0;
+  bool degen = false;
+  int grid = 1;
+  MixedGraph* d_graphs = nullptr;
+  const uint32_t* d_crc_tab = nullptr;
+  SegParams sp = {};      // templates: key tables and decoder settings
+  MixedParams mp = {};
+  std::vector<TbLane*> lanes;
 };
 
 MixedGraph tb_make_graph(int bgn, int Zc, int iLS) {
@@ -345,32 +353,96 @@ MixedGraph tb_make_graph(int bgn, int Zc, int iLS) {
   return m;
 }
 
+void lane_free(TbLane* l) {
+  cudaFree(l->d_cws);
+  cudaFree(l->d_cb_key);
+  cudaFree(l->d_tb_first);
+  cudaFree(l->d_tb_err);
+  cudaFree(l->d_items);
+  cudaFree(l->d_slots);
+  cudaFree(l->d_num_items);
+  cudaFree(l->d_counter);
+  cudaFree(l->d_cb_bits);
+  cudaFree(l->d_cb_status);
+  cudaFree(l->d_cb_iters);
+  cudaFree(l->d_scratch);
+  delete l;
+}
+
 void engine_free(TbEngine* e) {
+  for (TbLane* l : e->lanes) lane_free(l);
   cudaFree(e->d_graphs);
-  cudaFree(e->d_cws);
-  cudaFree(e->d_cb_key);
-  cudaFree(e->d_tb_first);
-  cudaFree(e->d_tb_err);
-  cudaFree(e->d_items);
-  cudaFree(e->d_slots);
-  cudaFree(e->d_num_items);
-  cudaFree(e->d_counter);
-  cudaFree(e->d_cb_bits);
-  cudaFree(e->d_cb_status);
-  cudaFree(e->d_cb_iters);
-  cudaFree(e->d_scratch);
   delete e;
 }
 
-int engine_decode(TbEngine* e, const nrldpc_tb_t* d_tbs, int n, const int16_t* d_llr, uint8_t* d_out,
+// Allocate lanes until the engine has n of them.
+int engine_lanes(TbEngine* e, int n) {
+  while ((int)e->lanes.size() < n) {
+    TbLane* l = new TbLane();
+    const int max_cbs = e->max_cbs, max_tbs = e->max_tbs;
+    const bool ok =
+        cudaMalloc(&l->d_cws, (size_t)max_cbs * sizeof(MixedCw)) == cudaSuccess &&
+        cudaMalloc(&l->d_cb_key, (size_t)max_cbs * sizeof(int32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_tb_first, (size_t)max_tbs * sizeof(int32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_tb_err, (size_t)max_tbs * sizeof(int32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_items, (size_t)e->max_items * sizeof(MixedItem)) == cudaSuccess &&
+        cudaMalloc(&l->d_slots, (size_t)e->max_slots * sizeof(int32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_num_items, 2 * sizeof(int32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_counter, sizeof(int32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_cb_bits, (size_t)max_cbs * kCbBitsStride) == cudaSuccess &&
+        cudaMalloc(&l->d_cb_status, (size_t)max_cbs * sizeof(int32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_cb_iters, (size_t)max_cbs * sizeof(int32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_scratch, (size_t)e->grid * kScratchWordsPerCta * sizeof(uint32_t)) == cudaSuccess &&
+        cudaMemset(l->d_num_items, 0, 2 * sizeof(int32_t)) == cudaSuccess;
+    if (!ok) {
+      lane_free(l);
+      return NRLDPC_ERR_CUDA;
+    }
+    SegParams& sp = l->sp;
+    sp = e->sp;
+    sp.cws = l->d_cws;
+    sp.cb_key = l->d_cb_key;
+    sp.tb_first = l->d_tb_first;
+    sp.tb_err = l->d_tb_err;
+    sp.items = l->d_items;
+    sp.slots = l->d_slots;
+    sp.num_items = l->d_num_items;
+    sp.counter = l->d_counter;
+    MixedParams& p = l->mp;
+    p = e->mp;
+    p.items = l->d_items;
+    p.slots = l->d_slots;
+    p.cws = l->d_cws;
+    p.num_items_dev = l->d_num_items;
+    p.counter = l->d_counter;
+    p.bits = l->d_cb_bits;
+    p.status = l->d_cb_status;
+    p.iters = l->d_cb_iters;
+    p.scratch = l->d_scratch;
+    FinishParams& fp = l->fp;
+    fp.tb_first = l->d_tb_first;
+    fp.tb_err = l->d_tb_err;
+    fp.batch_err = l->d_num_items + 1;
+    fp.cb_bits = l->d_cb_bits;
+    fp.cb_status = l->d_cb_status;
+    fp.cb_iters = l->d_cb_iters;
+    fp.crc24a_tab = e->d_crc_tab + (size_t)1 * kMaxB;
+    e->lanes.push_back(l);
+  }
+  return NRLDPC_OK;
+}
+
+int engine_decode(TbEngine* e, int lane, const nrldpc_tb_t* d_tbs, int n, const int16_t* d_llr, uint8_t* d_out,
                   int32_t* d_status, int32_t* d_iters, int16_t* d_harq, cudaStream_t s) {
   if (n == 0) return NRLDPC_OK;
-  tb_segment_kernel<<<1, kSegThreads, 0, s>>>(d_tbs, n, e->sp);
+  TbLane* l = e->lanes[lane];
+  tb_segment_kernel<<<1, kSegThreads, 0, s>>>(d_tbs, n, l->sp);
   count_launch();
-  e->mp.llr = d_llr;
-  e->mp.harq = d_harq;
-  if (launch_mixed(e->mp, e->grid, e->degen, s) != 0) return NRLDPC_ERR_CUDA;
-  FinishParams fp = e->fp;
+  MixedParams mp = l->mp;
+  mp.llr = d_llr;
+  mp.harq = d_harq;
+  if (launch_mixed(mp, e->grid, e->degen, s) != 0) return NRLDPC_ERR_CUDA;
+  FinishParams fp = l->fp;
   fp.out = d_out;
   fp.status = d_status;
   fp.iters = d_iters;
@@ -471,51 +543,21 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
   if (occ < 1) occ = 1;
   e->grid = std::max(1, std::min(2, occ) * e->num_sms);
   bool ok = cudaMalloc(&e->d_graphs, kKeys * sizeof(MixedGraph)) == cudaSuccess &&
-            cudaMalloc(&e->d_cws, (size_t)max_cbs * sizeof(MixedCw)) == cudaSuccess &&
-            cudaMalloc(&e->d_cb_key, (size_t)max_cbs * sizeof(int32_t)) == cudaSuccess &&
-            cudaMalloc(&e->d_tb_first, (size_t)max_tbs * sizeof(int32_t)) == cudaSuccess &&
-            cudaMalloc(&e->d_tb_err, (size_t)max_tbs * sizeof(int32_t)) == cudaSuccess &&
-            cudaMalloc(&e->d_items, (size_t)e->max_items * sizeof(MixedItem)) == cudaSuccess &&
-            cudaMalloc(&e->d_slots, (size_t)e->max_slots * sizeof(int32_t)) == cudaSuccess &&
-            cudaMalloc(&e->d_num_items, 2 * sizeof(int32_t)) == cudaSuccess &&
-            cudaMalloc(&e->d_counter, sizeof(int32_t)) == cudaSuccess &&
-            cudaMalloc(&e->d_cb_bits, (size_t)max_cbs * kCbBitsStride) == cudaSuccess &&
-            cudaMalloc(&e->d_cb_status, (size_t)max_cbs * sizeof(int32_t)) == cudaSuccess &&
-            cudaMalloc(&e->d_cb_iters, (size_t)max_cbs * sizeof(int32_t)) == cudaSuccess &&
-            cudaMalloc(&e->d_scratch, (size_t)e->grid * kScratchWordsPerCta * sizeof(uint32_t)) == cudaSuccess &&
             cudaMemcpy(e->d_graphs, graphs.data(), kKeys * sizeof(MixedGraph), cudaMemcpyHostToDevice) ==
                 cudaSuccess &&
-            cudaMemset(e->d_num_items, 0, 2 * sizeof(int32_t)) == cudaSuccess &&
             device_crc_table(&e->d_crc_tab) == NRLDPC_OK;
   if (!ok) {
     engine_free(e);
     return NRLDPC_ERR_CUDA;
   }
   SegParams& sp = e->sp;
-  sp.cws = e->d_cws;
-  sp.cb_key = e->d_cb_key;
-  sp.tb_first = e->d_tb_first;
-  sp.tb_err = e->d_tb_err;
-  sp.items = e->d_items;
-  sp.slots = e->d_slots;
-  sp.num_items = e->d_num_items;
-  sp.counter = e->d_counter;
   sp.max_cbs = max_cbs;
   sp.max_items = e->max_items;
   sp.max_slots = e->max_slots;
   MixedParams& p = e->mp;
   p.graphs = e->d_graphs;
-  p.items = e->d_items;
-  p.slots = e->d_slots;
-  p.cws = e->d_cws;
   p.num_items = 0;
-  p.num_items_dev = e->d_num_items;
-  p.counter = e->d_counter;
-  p.bits = e->d_cb_bits;
-  p.status = e->d_cb_status;
-  p.iters = e->d_cb_iters;
   p.crc_tab = e->d_crc_tab;
-  p.scratch = e->d_scratch;
   p.scratch_words = kScratchWordsPerCta;
   p.max_it = dc->max_iterations;
   p.fill = dc->filling_bit_value;
@@ -533,14 +575,10 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
       return NRLDPC_ERR_CUDA;
     }
   }
-  FinishParams& fp = e->fp;
-  fp.tb_first = e->d_tb_first;
-  fp.tb_err = e->d_tb_err;
-  fp.batch_err = e->d_num_items + 1;
-  fp.cb_bits = e->d_cb_bits;
-  fp.cb_status = e->d_cb_status;
-  fp.cb_iters = e->d_cb_iters;
-  fp.crc24a_tab = e->d_crc_tab + (size_t)1 * kMaxB;
+  if (engine_lanes(e, 1) != NRLDPC_OK) {
+    engine_free(e);
+    return NRLDPC_ERR_CUDA;
+  }
   if (prepare_mixed(e->degen) != 0) {
     engine_free(e);
     return NRLDPC_ERR_CUDA;
@@ -563,7 +601,7 @@ int32_t nrldpc_tb_engine_decode(void* engine, const nrldpc_tb_t* d_tbs, int32_t 
   if (!e || num_tbs < 0 || num_tbs > e->max_tbs) return NRLDPC_ERR_ARG;
   if (num_tbs == 0) return NRLDPC_OK;
   if (!d_tbs || !d_llr || !d_out || !d_status) return NRLDPC_ERR_ARG;
-  return engine_decode(e, d_tbs, num_tbs, d_llr, d_out, d_status, d_iterations, d_harq,
+  return engine_decode(e, 0, d_tbs, num_tbs, d_llr, d_out, d_status, d_iterations, d_harq,
                        reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -571,10 +609,11 @@ int32_t nrldpc_tb_engine_views(void* engine, const uint8_t** d_cb_bits, const in
                                const int32_t** d_cb_iterations, const int32_t** d_tb_first_cb) {
   TbEngine* e = static_cast<TbEngine*>(engine);
   if (!e) return NRLDPC_ERR_ARG;
-  if (d_cb_bits) *d_cb_bits = e->d_cb_bits;
-  if (d_cb_status) *d_cb_status = e->d_cb_status;
-  if (d_cb_iterations) *d_cb_iterations = e->d_cb_iters;
-  if (d_tb_first_cb) *d_tb_first_cb = e->d_tb_first;
+  const TbLane* l = e->lanes[0];
+  if (d_cb_bits) *d_cb_bits = l->d_cb_bits;
+  if (d_cb_status) *d_cb_status = l->d_cb_status;
+  if (d_cb_iterations) *d_cb_iterations = l->d_cb_iters;
+  if (d_tb_first_cb) *d_tb_first_cb = l->d_tb_first;
   return NRLDPC_OK;
 }
 
@@ -590,22 +629,32 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
   for (int i = 1; i < n; ++i)
     if (arrival_s[i] < arrival_s[i - 1]) return NRLDPC_ERR_ARG;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  // per in-flight slot: pinned descriptors and verdicts, device descriptors, completion event
+  // Per in-flight slot: its own stream and engine lane (so a new batch starts
+  // while earlier ones still decode, on SMs they leave free), pinned
+  // descriptors and verdicts, device descriptors, a completion event.
   struct Slot {
     nrldpc_tb_t* h_tbs = nullptr;
     int32_t* h_status = nullptr;
     nrldpc_tb_t* d_tbs = nullptr;
     int32_t* d_status = nullptr;
+    cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
     std::vector<int> members;
   };
   std::vector<Slot> slots(depth);
-  int rc = NRLDPC_OK;
+  int rc = engine_lanes(e, depth);
+  cudaEvent_t start = nullptr;
+  if (rc == NRLDPC_OK && (cudaEventCreateWithFlags(&start, cudaEventDisableTiming) != cudaSuccess ||
+                          cudaEventRecord(start, s) != cudaSuccess))
+    rc = NRLDPC_ERR_CUDA;
   for (Slot& sl : slots) {
+    if (rc != NRLDPC_OK) break;
     if (cudaMallocHost(&sl.h_tbs, (size_t)max_tbs * sizeof(nrldpc_tb_t)) != cudaSuccess ||
         cudaMallocHost(&sl.h_status, (size_t)max_tbs * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&sl.d_tbs, (size_t)max_tbs * sizeof(nrldpc_tb_t)) != cudaSuccess ||
         cudaMalloc(&sl.d_status, (size_t)max_tbs * sizeof(int32_t)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamWaitEvent(sl.stream, start, 0) != cudaSuccess ||   // after the caller's queued work
         cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess)
       rc = NRLDPC_ERR_CUDA;
   }
@@ -620,7 +669,7 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
   nrldpc_serve_stats_t st;
   memset(&st, 0, sizeof(st));
   std::deque<int> ready;
-  std::deque<int> inflight;   // slot indices in launch order
+  std::vector<int> inflight;   // slot indices
   std::vector<int> free_slots;
   for (int k = depth - 1; k >= 0; --k) free_slots.push_back(k);
   int64_t budget_used = 0;
@@ -638,11 +687,14 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
       break;
     }
     bool progress = false;
-    // completions, in launch order
-    while (!inflight.empty()) {
-      Slot& sl = slots[inflight.front()];
+    // completions (batches on different streams may finish in any order)
+    for (size_t q_i = 0; q_i < inflight.size();) {
+      Slot& sl = slots[inflight[q_i]];
       const cudaError_t q = cudaEventQuery(sl.ev);
-      if (q == cudaErrorNotReady) break;
+      if (q == cudaErrorNotReady) {
+        ++q_i;
+        continue;
+      }
       if (q != cudaSuccess) {
         rc = NRLDPC_ERR_CUDA;
         break;
@@ -658,8 +710,8 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
         done++;
       }
       t_last = tv;
-      free_slots.push_back(inflight.front());
-      inflight.pop_front();
+      free_slots.push_back(inflight[q_i]);
+      inflight.erase(inflight.begin() + q_i);
       progress = true;
     }
     if (rc != NRLDPC_OK) break;
@@ -698,12 +750,13 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
         cbs += ncb[i];
       }
       const int m = (int)sl.members.size();
-      if (cudaMemcpyAsync(sl.d_tbs, sl.h_tbs, (size_t)m * sizeof(nrldpc_tb_t), cudaMemcpyHostToDevice, s) !=
+      cudaStream_t ss = sl.stream;
+      if (cudaMemcpyAsync(sl.d_tbs, sl.h_tbs, (size_t)m * sizeof(nrldpc_tb_t), cudaMemcpyHostToDevice, ss) !=
               cudaSuccess ||
-          engine_decode(e, sl.d_tbs, m, d_llr, d_out, sl.d_status, nullptr, nullptr, s) != NRLDPC_OK ||
-          cudaMemcpyAsync(sl.h_status, sl.d_status, (size_t)m * sizeof(int32_t), cudaMemcpyDeviceToHost, s) !=
+          engine_decode(e, k, sl.d_tbs, m, d_llr, d_out, sl.d_status, nullptr, nullptr, ss) != NRLDPC_OK ||
+          cudaMemcpyAsync(sl.h_status, sl.d_status, (size_t)m * sizeof(int32_t), cudaMemcpyDeviceToHost, ss) !=
               cudaSuccess ||
-          cudaEventRecord(sl.ev, s) != cudaSuccess) {
+          cudaEventRecord(sl.ev, ss) != cudaSuccess) {
         rc = NRLDPC_ERR_CUDA;
         break;
       }
@@ -714,15 +767,23 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
     }
     if (!progress) std::this_thread::yield();
   }
-  // leave nothing in flight that references the slot buffers
-  cudaStreamSynchronize(s);
+  // leave nothing in flight that references the slot buffers; later work on
+  // the caller's stream comes after every batch
+  for (Slot& sl : slots) {
+    if (sl.stream) {
+      cudaStreamSynchronize(sl.stream);
+      if (sl.ev && cudaEventRecord(sl.ev, sl.stream) == cudaSuccess) cudaStreamWaitEvent(s, sl.ev, 0);
+    }
+  }
   for (Slot& sl : slots) {
     cudaFreeHost(sl.h_tbs);
     cudaFreeHost(sl.h_status);
     cudaFree(sl.d_tbs);
     cudaFree(sl.d_status);
     if (sl.ev) cudaEventDestroy(sl.ev);
+    if (sl.stream) cudaStreamDestroy(sl.stream);
   }
+  if (start) cudaEventDestroy(start);
   st.wall_s = t_last - t0 - (n > 0 ? arrival_s[0] : 0.0);
   st.mean_batch_tbs = st.batches ? batch_tbs_sum / (double)st.batches : 0.0;
   if (stats) *stats = st;
