@@ -615,7 +615,8 @@ def run_serve(args):
         arrivals = np.cumsum(rng.exponential(1.0 / lam, n_arr))
         with torch.cuda.stream(stream):
             res = tbm.serve(eng, trace, arrivals, arena, out, max_batch_tbs=8192, max_batch_cbs=65536,
-                            llr_budget_bytes=4 << 30, pipeline_depth=2, timeout_s=120.0, stream=stream)
+                            llr_budget_bytes=4 << 30, pipeline_depth=args.pipeline_depth, timeout_s=120.0,
+                            stream=stream)
         done = res.status >= 0
         lat = res.latency_s[done] * 1e3
         bits_ok = float(A_bits[pick][res.status == 0].sum())
@@ -638,7 +639,7 @@ def run_serve(args):
                     "per-block Es/N0 uniform in +-1.5 dB around the MCS's measured 10 % code-block error point",
             "config": {"workload": f"serving: pool of {n_pool} transport blocks ({int(n_cbs.sum())} code blocks, "
                                    f"{pool_gbit:.3f} Gbit), Poisson arrivals 10k-200k TB/s, LLR budget 4 GiB, "
-                                   "algo 1 10 iterations with CRC early exit, continuous batching depth 2",
+                                   f"algo 1 10 iterations with CRC early exit, continuous batching depth {args.pipeline_depth}",
                        "parallelism": "single GPU"},
             "loads": loads,
             "offline_pool": {"engine_ms": round(ms_engine, 3), "engine_gbit_per_s": round(pool_gbit / ms_engine * 1e3, 4),
@@ -772,6 +773,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n-cw", type=int, default=N_CW, help="code blocks per step (profiling runs use fewer)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--pipeline-depth", type=int, default=6, help="serve: batches in flight (streams)")
     ap.add_argument("--workload", default="bg1_zc384", choices=["bg1_zc384", "mixed", "train", "serve"],
                     help="mixed: 32768 blocks over all 51 lifting sizes, BG1 60 %%, rate U[0.2, 0.92], Qm 2-8; "
                          "train: learned min-sum forward+backward, batch 4096, 10 iterations")
