@@ -10,7 +10,8 @@
 // Mapping (B200-first, not the reference's <<<1, Zc>>> launch):
 //  * Two code blocks of the same (BG, Zc) are interleaved as int16x2 in every
 //    32-bit word, so each check-node step is one packed dual-int16 SIMD op for
-//    both code blocks (__vsub2 / __vabsss2 / __vibmin_s16x2 / __vaddss2 ...).
+//    both code blocks (__vsub2 / __vmaxs2 / __vibmin_u16x2 / __vadd2 ..., see
+//    nrldpc_fixed_row.cuh).
 //  * Lifted row zx of every layer is owned by one thread; a CTA holds G pairs
 //    (G = floor(384 / Zc)) so small lifting sizes still fill the CTA.
 //  * The beliefs LQ of all G pairs live in shared memory for the whole decode.
