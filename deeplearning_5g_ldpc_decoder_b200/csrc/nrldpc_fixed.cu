@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
           const int32_t alpha = (int32_t)(int16_t)(ab & 0xFFFFu);
           const int32_t beta = ((int32_t)ab) >> 16;
           layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0, alpha, beta,
-                                     it == 0, scratch + p.lr_off[row] + tid);
+                                           alpha, beta, it == 0 ? 0xFFFFFFFFu : 0u, scratch + p.lr_off[row] + tid);
         }
         __syncthreads();
       }

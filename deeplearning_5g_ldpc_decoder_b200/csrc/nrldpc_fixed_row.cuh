@@ -30,10 +30,13 @@ __device__ __forceinline__ uint32_t scale_half(int32_t m, int32_t alpha, int32_t
   const int32_t s = (alpha * off + (1 << 14)) >> 15;
   return (uint32_t)s & 0xFFFFu;
 }
-__device__ __forceinline__ uint32_t scale_pair(uint32_t c, int32_t alpha, int32_t beta) {
+// Both halves, each with its own (alpha, beta): the two code blocks of a lane
+// pair may be at different iterations of an iteration-dependent table (algo 2).
+__device__ __forceinline__ uint32_t scale_pair(uint32_t c, int32_t alpha0, int32_t beta0, int32_t alpha1,
+                                               int32_t beta1) {
   const int32_t lo = (int32_t)(int16_t)(c & 0xFFFFu);
   const int32_t hi = ((int32_t)c) >> 16;
-  return scale_half(lo, alpha, beta) | (scale_half(hi, alpha, beta) << 16);
+  return scale_half(lo, alpha0, beta0) | (scale_half(hi, alpha1, beta1) << 16);
 }
 
 // clip_llr (c_lib/fixedpoint_ldpc_decoder.c:28-36) of the exact int32 sum, for
@@ -66,6 +69,9 @@ __device__ __forceinline__ uint32_t cond_neg16x2(uint32_t v, uint32_t m) { retur
 //        "carries new_min2" bits at bits j-12 / j+4.
 // Edge j's message is  flip ? -v : v  with  v = carries_min2 ? new_min2 : new_min1,
 // which is exactly the reference's sel_lr[j] = (int16)(+-sign * new_val).
+// Every word keeps block 0's fields in bits 0-15 and block 1's in bits 16-31,
+// so `fresh` (0xFFFF per half that starts its first iteration) clears one
+// block's old message without touching the other's.
 //
 // Instruction budget: packed add/sub run on the FMA pipe, packed min/max,
 // PRMT and LOP3 on the ALU pipe (the bottleneck); the emulated saturating
@@ -73,16 +79,25 @@ __device__ __forceinline__ uint32_t cond_neg16x2(uint32_t v, uint32_t m) { retur
 template <int D, bool kDegenClip, bool kSmemEdges, typename P>
 __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__ sedges, char* __restrict__ lqs, uint32_t zx4,
                                            uint32_t zxm4, uint32_t gb4, int e0, int32_t alpha, int32_t beta,
-                                           bool first, uint32_t* __restrict__ lrp) {
+                                           int32_t alpha1, int32_t beta1, uint32_t fresh,
+                                           uint32_t* __restrict__ lrp) {
   constexpr int J = D < 16 ? D : 16;
   constexpr int S = kThreadsTarget;    // plane stride (words)
   uint32_t n1 = 0u, n2 = 0u, xf = 0u, xi = 0u, y = 0u;
-  if (!first) {
+  if (fresh != 0xFFFFFFFFu) {
     n1 = lrp[0];
     n2 = lrp[S];
     xf = lrp[2 * S];
     xi = lrp[3 * S];
     if (D > 16) y = lrp[4 * S];
+    if (fresh) {
+      const uint32_t keep = ~fresh;
+      n1 &= keep;
+      n2 &= keep;
+      xf &= keep;
+      xi &= keep;
+      y &= keep;
+    }
   }
 
   uint32_t rel[D];
@@ -132,8 +147,8 @@ __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__
   // Clip the minima (both <= 32767) to max_llr, then offset/normalise (:121-126).
   const uint32_t maxp = ((uint32_t)(uint16_t)p.max_llr) * 0x10001u;
   const uint32_t minp = ((uint32_t)(uint16_t)p.min_llr) * 0x10001u;
-  const uint32_t s1 = scale_pair(__vmins2(m1, maxp), alpha, beta);
-  const uint32_t s2 = scale_pair(__vmins2(m2, maxp), alpha, beta);
+  const uint32_t s1 = scale_pair(__vmins2(m1, maxp), alpha, beta, alpha1, beta1);
+  const uint32_t s2 = scale_pair(__vmins2(m2, maxp), alpha, beta, alpha1, beta1);
   const uint32_t XI = (oh0 & 0xFFFFu) | (oh1 << 16);
   uint32_t XF = 0u;
   uint32_t Y = 0u;
@@ -194,11 +209,11 @@ __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__
 
 template <bool kDegenClip, bool kSmemEdges, typename P>
 __device__ __forceinline__ void layer_dispatch(int deg, const P& p, const uint2* sedges, char* lqs, uint32_t zx4, uint32_t zxm4,
-                                               uint32_t gb4, int e0, int32_t alpha, int32_t beta, bool first,
-                                               uint32_t* lrp) {
+                                               uint32_t gb4, int e0, int32_t alpha, int32_t beta,
+                                               int32_t alpha1, int32_t beta1, uint32_t fresh, uint32_t* lrp) {
   switch (deg) {
 #define NRLDPC_ROW(D) \
-  case D: row_update<D, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, first, lrp); break;
+  case D: row_update<D, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, alpha1, beta1, fresh, lrp); break;
     NRLDPC_ROW(3)
     NRLDPC_ROW(4)
     NRLDPC_ROW(5)
@@ -208,7 +223,7 @@ __device__ __forceinline__ void layer_dispatch(int deg, const P& p, const uint2*
     NRLDPC_ROW(9)
     NRLDPC_ROW(10)
 #undef NRLDPC_ROW
-    default: row_update<19, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, first, lrp); break;
+    default: row_update<19, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, alpha1, beta1, fresh, lrp); break;
   }
 }
 

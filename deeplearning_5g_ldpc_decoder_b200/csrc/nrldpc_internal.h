@@ -128,14 +128,19 @@ struct MixedCw {
   int32_t harq_mode;  // bit 0: add to the stored soft buffer, bit 1: store the soft buffer
   int64_t harq_off;   // elements into the soft-buffer arena (N + 2Zc of them), when harq_mode != 0
 };
-// One work item: up to G pairs of one (BG, Zc); slots[slot_base + 2g + h] = block or -1.
+// One work item: a CTA's claim on the blocks of one (BG, Zc).  The CTA takes
+// up to 2G blocks from that graph's queue and refills each int16 half lane from
+// the same queue as soon as its block finishes.
 struct MixedItem {
-  int32_t graph, slot_base, npairs, bmax_pad;
+  int32_t graph, pad0, pad1, pad2;
 };
 struct MixedParams {
   const MixedGraph* graphs;
   const MixedItem* items;
-  const int32_t* slots;
+  const int32_t* cb_list;              // blocks grouped by graph: cb_list[key_base[k] .. + key_count[k])
+  const int32_t* key_base;             // per graph
+  const int32_t* key_count;            // per graph (device-built when num_items_dev is set)
+  int32_t* key_cursor;                 // per graph: next unclaimed entry, zeroed before each launch
   const MixedCw* cws;
   int32_t num_items;
   const int32_t* num_items_dev;        // when set, the item count is read from the device (built there)

@@ -4,11 +4,17 @@
 //
 // Same arithmetic as the uniform kernel (nrldpc_fixed_row.cuh, bit-exact with
 // c_lib/fixedpoint_ldpc_decoder.c).  Differences:
-//  * work items (G pairs of one (BG, Zc)) come from a device work queue
-//    (atomic counter), so CTAs stay busy whatever the size mix;
-//  * the item's base-graph tables (per-edge shared-memory offsets, row offsets,
-//    scratch layout) are staged into shared memory per item;
-//  * the two code blocks of a pair share (BG, Zc) but may differ in every other
+//  * work items come from a device work queue (atomic counter); an item is a
+//    CTA's claim on one (BG, Zc), whose tables (per-edge shared-memory offsets,
+//    row offsets, scratch layout) are staged into shared memory;
+//  * the CTA takes up to 2G blocks of that graph from the graph's block queue
+//    (a second atomic cursor) and, whenever a block passes its CRC or reaches
+//    max_iterations, emits it and refills that int16 half lane with the next
+//    block of the queue: every block costs its own iterations, not the slowest
+//    block's of its CTA.  The refilled half starts from zero messages (the
+//    `fresh` mask) and its own iteration count, so each block decodes exactly
+//    as it would alone;
+//  * the two blocks of a lane pair share (BG, Zc) but may differ in every other
 //    parameter: rate recovery, the CRC check and the outputs use each block's
 //    own B, E, Qm, rv and CRC type.
 #include <cuda_runtime.h>
@@ -68,12 +74,35 @@ __device__ void mixed_emit(const MixedParams& p, const uint32_t* lq, int zx, int
   }
 }
 
+// Next block of graph `key`'s queue, or -1 when it is empty.
+__device__ __forceinline__ int take_block(const MixedParams& p, int key) {
+  const int i = atomicAdd(p.key_cursor + key, 1);
+  return i < p.key_count[key] ? p.cb_list[p.key_base[key] + i] : -1;
+}
+
+// Rate recovery of one block into half h of the group's LQ words (the other
+// half is kept), with its HARQ soft buffer.
+__device__ __forceinline__ void recover_half(const MixedParams& p, const MixedGraph& g, const MixedCw& c, int h,
+                                             uint32_t* lq, int zx) {
+  const int16_t* in = p.llr + c.llr_off;
+  int16_t* hq = (c.harq_mode && p.harq) ? p.harq + c.harq_off : nullptr;
+  const int shift = 16 * h;
+  const uint32_t keep = h ? 0x0000FFFFu : 0xFFFF0000u;
+  for (int i = zx; i < g.lq_len; i += g.Zc) {
+    const int32_t init = (hq && (c.harq_mode & 1)) ? hq[i] : 0;
+    const int32_t a = mixed_recover(g, c, in, i, p.fill, init);
+    if (hq && (c.harq_mode & 2)) hq[i] = (int16_t)a;
+    lq[i] = (lq[i] & keep) | (((uint32_t)a & 0xFFFFu) << shift);
+  }
+}
+
 template <bool kDegenClip>
 __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __grid_constant__ MixedParams p) {
   extern __shared__ __align__(16) uint32_t s_lq[];
   __shared__ uint32_t s_crc[2 * kMaxGroups];
   __shared__ MixedGraph s_g;
-  __shared__ int4 s_grp[kMaxGroups];      // per pair: B0, B1, CRC table offsets of both halves
+  __shared__ int4 s_grp[kMaxGroups];      // per group: B of both halves (0 when idle), CRC table offsets
+  __shared__ int s_cw[2 * kMaxGroups];    // block in each half lane, -1 when idle
   __shared__ int s_item;
 
   const int tid = threadIdx.x;
@@ -84,9 +113,9 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
     __syncthreads();
     const int item = s_item;
     if (item >= num_items) break;
-    const MixedItem desc = p.items[item];
+    const int key = p.items[item].graph;
     {
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(p.graphs + desc.graph);
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(p.graphs + key);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&s_g);
       for (int w = tid; w < (int)(sizeof(MixedGraph) / 4); w += blockDim.x) dst[w] = __ldg(src + w);
     }
@@ -96,57 +125,54 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
     const int zx = tid - g * Zc;
     const bool active = g < G;
     uint32_t* lq = s_lq + (active ? g : 0) * lq_len;
-    const int cw0 = active ? p.slots[desc.slot_base + 2 * g] : -1;
-    const int cw1 = active ? p.slots[desc.slot_base + 2 * g + 1] : -1;
-    const bool v0 = cw0 >= 0, v1 = cw1 >= 0;
-    MixedCw c0 = {}, c1 = {};
-    if (v0) c0 = p.cws[cw0];
-    if (v1) c1 = p.cws[cw1];
-    if (active && zx == 0)
-      s_grp[g] = make_int4(v0 ? c0.B : 0, v1 ? c1.B : 0, c0.crctype * kMaxB, c1.crctype * kMaxB);
-
+    if (tid < 2 * G) s_cw[tid] = take_block(p, key);
+    __syncthreads();
+    int cw[2] = {active ? s_cw[2 * g] : -1, active ? s_cw[2 * g + 1] : -1};
+    if (__syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0))) continue;   // the graph's queue is empty
+    MixedCw c[2];
+    c[0] = cw[0] >= 0 ? p.cws[cw[0]] : MixedCw{};
+    c[1] = cw[1] >= 0 ? p.cws[cw[1]] : MixedCw{};
+    int itv[2] = {0, 0};
     if (active) {
-      const int16_t* in0 = p.llr + c0.llr_off;
-      const int16_t* in1 = p.llr + c1.llr_off;
-      int16_t* h0 = (v0 && c0.harq_mode && p.harq) ? p.harq + c0.harq_off : nullptr;
-      int16_t* h1 = (v1 && c1.harq_mode && p.harq) ? p.harq + c1.harq_off : nullptr;
-      for (int i = zx; i < lq_len; i += Zc) {
-        const int32_t i0 = (h0 && (c0.harq_mode & 1)) ? h0[i] : 0;
-        const int32_t i1 = (h1 && (c1.harq_mode & 1)) ? h1[i] : 0;
-        const int32_t a0 = v0 ? mixed_recover(s_g, c0, in0, i, p.fill, i0) : 0;
-        const int32_t a1 = v1 ? mixed_recover(s_g, c1, in1, i, p.fill, i1) : 0;
-        if (h0 && (c0.harq_mode & 2)) h0[i] = (int16_t)a0;
-        if (h1 && (c1.harq_mode & 2)) h1[i] = (int16_t)a1;
-        lq[i] = ((uint32_t)a0 & 0xFFFFu) | ((uint32_t)a1 << 16);
-      }
+      if (zx == 0)
+        s_grp[g] = make_int4(cw[0] >= 0 ? c[0].B : 0, cw[1] >= 0 ? c[1].B : 0, c[0].crctype * kMaxB,
+                             c[1].crctype * kMaxB);
+      for (int i = zx; i < lq_len; i += Zc) lq[i] = 0u;
+      for (int h = 0; h < 2; ++h)
+        if (cw[h] >= 0) recover_half(p, s_g, c[h], h, lq, zx);
     }
     if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
-    bool done0 = !v0, done1 = !v1;
+    uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
     __syncthreads();
 
     const int bi = s_g.bgn == 1 ? 0 : 1;
     const uint32_t zx4 = 4u * (uint32_t)zx;
     const uint32_t zxm4 = zx4 - 4u * (uint32_t)Zc;
     const uint32_t gb4 = 4u * (uint32_t)((active ? g : 0) * lq_len);
-    const int Bp = desc.bmax_pad;
-    int it = 0;
-    for (; it < p.max_it; ++it) {
-      for (int row = 0; row < s_g.R; ++row) {
+    const int Bp = (s_g.K + 31) & ~31;   // every block's B <= K
+    for (;;) {
+      const bool run = p.max_it > 0;   // max_iterations == 0: rate recovery only, status 1
+      for (int row = 0; run && row < s_g.R; ++row) {
         if (active) {
           const int e0 = s_g.row_off[row];
           const int deg = s_g.row_off[row + 1] - e0;
-          const uint32_t ab = p.weights_T[bi] > 0
-                                  ? __ldg(p.weights[bi] + (min(it, p.weights_T[bi] - 1) * s_g.R + row))
-                                  : p.w_inline[bi][row];
-          const int32_t alpha = (int32_t)(int16_t)(ab & 0xFFFFu);
-          const int32_t beta = ((int32_t)ab) >> 16;
-          layer_dispatch<kDegenClip, true>(deg, p, s_g.edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0, alpha,
-                                           beta, it == 0, scratch + s_g.lr_off[row] + tid);
+          uint32_t ab0, ab1;
+          if (p.weights_T[bi] > 0) {
+            ab0 = __ldg(p.weights[bi] + (min(itv[0], p.weights_T[bi] - 1) * s_g.R + row));
+            ab1 = __ldg(p.weights[bi] + (min(itv[1], p.weights_T[bi] - 1) * s_g.R + row));
+          } else {
+            ab0 = ab1 = p.w_inline[bi][row];
+          }
+          layer_dispatch<kDegenClip, true>(deg, p, s_g.edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0,
+                                           (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
+                                           (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, fresh,
+                                           scratch + s_g.lr_off[row] + tid);
         }
         __syncthreads();
       }
-      // Hard decisions + CRC of both halves of every pair (each with its own B and CRC type).
-      for (int k = tid; k < G * Bp; k += blockDim.x) {
+      fresh = 0u;
+      // Hard decisions + CRC of both halves of every group (each with its own B and CRC type).
+      for (int k = tid; run && k < G * Bp; k += blockDim.x) {
         const int gg = k / Bp;
         const int i = k - gg * Bp;
         const int4 gr = s_grp[gg];
@@ -162,26 +188,41 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
         }
       }
       __syncthreads();
+      bool refill[2] = {false, false};
       if (active) {
-        const bool pass0 = !done0 && s_crc[2 * g] == 0u;
-        const bool pass1 = !done1 && s_crc[2 * g + 1] == 0u;
-        if (pass0) mixed_emit(p, lq, zx, Zc, cw0, c0, 0, 0, it + 1);
-        if (pass1) mixed_emit(p, lq, zx, Zc, cw1, c1, 1, 0, it + 1);
-        done0 = done0 || pass0;
-        done1 = done1 || pass1;
+        for (int h = 0; h < 2; ++h) {
+          if (cw[h] < 0) continue;
+          if (run) ++itv[h];
+          const bool pass = run && s_crc[2 * g + h] == 0u;
+          if (pass || itv[h] >= p.max_it) {
+            mixed_emit(p, lq, zx, Zc, cw[h], c[h], h, pass ? 0 : 1, itv[h]);
+            refill[h] = true;
+          }
+        }
       }
-      const bool all_done = __syncthreads_and(done0 && done1);
+      __syncthreads();   // s_crc read and emits done before the lanes are refilled
       if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
-      if (all_done) {
-        ++it;
-        break;
+      if (active && zx == 0)
+        for (int h = 0; h < 2; ++h)
+          if (refill[h]) s_cw[2 * g + h] = take_block(p, key);
+      __syncthreads();
+      if (active) {
+        for (int h = 0; h < 2; ++h) {
+          if (!refill[h]) continue;
+          cw[h] = s_cw[2 * g + h];
+          itv[h] = 0;
+          if (cw[h] >= 0) {
+            c[h] = p.cws[cw[h]];
+            recover_half(p, s_g, c[h], h, lq, zx);
+            fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
+          }
+        }
+        if (zx == 0 && (refill[0] || refill[1]))
+          s_grp[g] = make_int4(cw[0] >= 0 ? c[0].B : 0, cw[1] >= 0 ? c[1].B : 0, c[0].crctype * kMaxB,
+                               c[1].crctype * kMaxB);
       }
+      if (__syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0))) break;
     }
-    if (active) {
-      if (!done0) mixed_emit(p, lq, zx, Zc, cw0, c0, 0, 1, it);
-      if (!done1) mixed_emit(p, lq, zx, Zc, cw1, c1, 1, 1, it);
-    }
-    __syncthreads();   // shared state is reused by the next item
   }
 }
 

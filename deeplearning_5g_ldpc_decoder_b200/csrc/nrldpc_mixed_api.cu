@@ -26,10 +26,10 @@ struct MixedPlanImpl {
   MixedGraph* d_graphs = nullptr;
   MixedCw* d_cws = nullptr;
   MixedItem* d_items = nullptr;
-  int32_t* d_slots = nullptr;
-  int32_t* d_counter = nullptr;
+  int32_t* d_queue = nullptr;     // block queues: cb_list, then key_base, key_count
+  int32_t* d_counter = nullptr;   // work-item head, then one cursor per graph
   uint32_t* d_scratch = nullptr;
-  size_t items_cap = 0, slots_cap = 0;
+  size_t items_cap = 0;
   int scratch_ctas = 0;
   MixedParams params = {};
   int order = 0;          // 0: largest work first, 1: graphs interleaved
@@ -49,7 +49,7 @@ void free_plan(MixedPlanImpl* pl) {
   cudaFree(pl->d_graphs);
   cudaFree(pl->d_cws);
   cudaFree(pl->d_items);
-  cudaFree(pl->d_slots);
+  cudaFree(pl->d_queue);
   cudaFree(pl->d_counter);
   cudaFree(pl->d_scratch);
   delete pl;
@@ -79,7 +79,9 @@ MixedGraph make_graph(int bgn, int Zc, int iLS) {
   return m;
 }
 
-// Work items for the current order; uploads items + slots.
+// Work items for the current order: per graph, one claim per G lane pairs of
+// its blocks (a CTA refills its lanes from the graph's queue, so a claim may
+// end up with more blocks than 2G or, when other CTAs drained the queue, none).
 int build_items(MixedPlanImpl* pl) {
   struct It {
     MixedItem m;
@@ -87,28 +89,16 @@ int build_items(MixedPlanImpl* pl) {
     int graph_rank;
   };
   std::vector<It> items;
-  std::vector<int32_t> slots;
   for (size_t gi = 0; gi < pl->graphs.size(); ++gi) {
     const MixedGraph& g = pl->graphs[gi];
     const BaseGraph& bg = base_graph(g.bgn);
-    const std::vector<int>& mem = pl->members[gi];
-    const int npairs_total = ((int)mem.size() + 1) / 2;
+    const int npairs_total = ((int)pl->members[gi].size() + 1) / 2;
     int rank = 0;
     for (int p0 = 0; p0 < npairs_total; p0 += g.G, ++rank) {
       It it;
+      memset(&it.m, 0, sizeof(it.m));
       it.m.graph = (int32_t)gi;
-      it.m.slot_base = (int32_t)slots.size();
-      it.m.npairs = std::min(g.G, npairs_total - p0);
-      int bmax = 0;
-      for (int k = 0; k < 2 * g.G; ++k) {
-        const int idx = 2 * p0 + k;
-        const bool in = k < 2 * it.m.npairs && idx < (int)mem.size();
-        const int cw = in ? mem[idx] : -1;
-        slots.push_back(cw);
-        if (cw >= 0) bmax = std::max(bmax, pl->cws[cw].B);
-      }
-      it.m.bmax_pad = (bmax + 31) & ~31;
-      it.cost = (double)bg.nnz * g.Zc * it.m.npairs;
+      it.cost = (double)bg.nnz * g.Zc * std::min(g.G, npairs_total - p0);
       it.graph_rank = rank;
       items.push_back(it);
     }
@@ -125,16 +115,9 @@ int build_items(MixedPlanImpl* pl) {
     if (cudaMalloc(&pl->d_items, host.size() * sizeof(MixedItem)) != cudaSuccess) return NRLDPC_ERR_CUDA;
     pl->items_cap = host.size();
   }
-  if (slots.size() > pl->slots_cap) {
-    cudaFree(pl->d_slots);
-    if (cudaMalloc(&pl->d_slots, slots.size() * sizeof(int32_t)) != cudaSuccess) return NRLDPC_ERR_CUDA;
-    pl->slots_cap = slots.size();
-  }
-  if (cudaMemcpy(pl->d_items, host.data(), host.size() * sizeof(MixedItem), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(pl->d_slots, slots.data(), slots.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+  if (cudaMemcpy(pl->d_items, host.data(), host.size() * sizeof(MixedItem), cudaMemcpyHostToDevice) != cudaSuccess)
     return NRLDPC_ERR_CUDA;
   pl->params.items = pl->d_items;
-  pl->params.slots = pl->d_slots;
   pl->params.num_items = (int32_t)host.size();
   return NRLDPC_OK;
 }
@@ -161,7 +144,9 @@ int configure(MixedPlanImpl* pl, int ctas_per_sm, int order) {
 }
 
 int enqueue(MixedPlanImpl* pl, cudaStream_t s) {
-  if (cudaMemsetAsync(pl->params.counter, 0, sizeof(int32_t), s) != cudaSuccess) return NRLDPC_ERR_CUDA;
+  // work-item head and every graph's queue cursor start at zero
+  if (cudaMemsetAsync(pl->params.counter, 0, sizeof(int32_t) * (1 + pl->graphs.size()), s) != cudaSuccess)
+    return NRLDPC_ERR_CUDA;
   return launch_mixed(pl->params, pl->grid, pl->degen, s) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
 }
 
@@ -275,17 +260,34 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
       return NRLDPC_ERR_CUDA;
     }
   }
+  // per-graph block queues: members of each graph in pairing order
+  std::vector<int32_t> queue;
+  std::vector<int32_t> base(pl->graphs.size()), count(pl->graphs.size());
+  for (size_t gi = 0; gi < pl->graphs.size(); ++gi) {
+    base[gi] = (int32_t)queue.size();
+    count[gi] = (int32_t)pl->members[gi].size();
+    queue.insert(queue.end(), pl->members[gi].begin(), pl->members[gi].end());
+  }
+  const size_t ng = pl->graphs.size();
+  queue.insert(queue.end(), base.begin(), base.end());
+  queue.insert(queue.end(), count.begin(), count.end());
   if (device_crc_table(&p.crc_tab) != NRLDPC_OK ||
       cudaMalloc(&pl->d_graphs, pl->graphs.size() * sizeof(MixedGraph)) != cudaSuccess ||
       cudaMalloc(&pl->d_cws, pl->cws.size() * sizeof(MixedCw)) != cudaSuccess ||
-      cudaMalloc(&pl->d_counter, sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc(&pl->d_counter, sizeof(int32_t) * (1 + ng)) != cudaSuccess ||
+      cudaMalloc(&pl->d_queue, sizeof(int32_t) * queue.size()) != cudaSuccess ||
       cudaMemcpy(pl->d_graphs, pl->graphs.data(), pl->graphs.size() * sizeof(MixedGraph), cudaMemcpyHostToDevice) !=
           cudaSuccess ||
       cudaMemcpy(pl->d_cws, pl->cws.data(), pl->cws.size() * sizeof(MixedCw), cudaMemcpyHostToDevice) !=
-          cudaSuccess) {
+          cudaSuccess ||
+      cudaMemcpy(pl->d_queue, queue.data(), sizeof(int32_t) * queue.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
     free_plan(pl);
     return NRLDPC_ERR_CUDA;
   }
+  p.cb_list = pl->d_queue;
+  p.key_base = pl->d_queue + (queue.size() - 2 * ng);
+  p.key_count = pl->d_queue + (queue.size() - ng);
+  p.key_cursor = pl->d_counter + 1;
   p.graphs = pl->d_graphs;
   p.cws = pl->d_cws;
   p.counter = pl->d_counter;

@@ -7,8 +7,9 @@
 // Per batch, three launches on one stream, no host synchronisation:
 //  1. tb_segment_kernel (one CTA): TS 38.212 5.2.2 segmentation of every
 //     transport block, per-code-block rate-recovery parameters, then the code
-//     blocks bucketed by (BG, Zc), paired into int16x2 lanes and grouped into
-//     work items for the mixed kernel (largest lifting sizes first);
+//     blocks bucketed by (BG, Zc) into one block queue per graph, and one work
+//     item per G lane pairs of each graph for the mixed kernel (largest
+//     lifting sizes first);
 //  2. fixed_mixed_kernel (nrldpc_mixed.cu), reading its item count from the
 //     device;
 //  3. tb_finish_kernel (one 512-thread CTA per transport block): code-block verdicts,
@@ -42,10 +43,13 @@ struct SegParams {
   int32_t* tb_first;
   int32_t* tb_err;        // per TB: tb_segment error (0 = valid)
   MixedItem* items;
-  int32_t* slots;
+  int32_t* cb_list;       // [max_cbs] code blocks grouped by graph key
+  int32_t* key_base;      // [kKeys] first cb_list entry of each key
+  int32_t* key_count;     // [kKeys] code blocks of each key
+  int32_t* key_cursor;    // [kKeys] queue cursors of the mixed kernel
   int32_t* num_items;     // [0] items of the batch, [1] batch error (1 = over capacity)
   int32_t* counter;       // work-queue head of the mixed kernel
-  int32_t max_cbs, max_items, max_slots;
+  int32_t max_cbs, max_items;
   int32_t key_G[kKeys];           // pairs per work item of each (BG, Zc)
   int16_t key_by_rank[kKeys];     // keys in descending work per block; -1 past the end
 };
@@ -53,8 +57,8 @@ struct SegParams {
 __global__ void __launch_bounds__(kSegThreads) tb_segment_kernel(const nrldpc_tb_t* __restrict__ tbs, int n,
                                                                  const __grid_constant__ SegParams sp) {
   __shared__ int s_scan[kSegThreads];
-  __shared__ int s_count[kKeys], s_cursor[kKeys], s_item_base[kKeys], s_slot_base[kKeys], s_items[kKeys];
-  __shared__ int s_total, s_num_items, s_num_slots, s_err;
+  __shared__ int s_count[kKeys], s_cursor[kKeys], s_item_base[kKeys], s_cb_base[kKeys], s_items[kKeys];
+  __shared__ int s_total, s_num_items, s_err;
   const int tid = threadIdx.x;
   if (tid < kKeys) {
     s_count[tid] = 0;
@@ -123,9 +127,9 @@ __global__ void __launch_bounds__(kSegThreads) tb_segment_kernel(const nrldpc_tb
     }
   }
   __syncthreads();
-  // 3. work items per (BG, Zc), largest lifting sizes first
+  // 3. block queues and work items per (BG, Zc), largest lifting sizes first
   if (tid == 0) {
-    int ib = 0, sb = 0;
+    int ib = 0, cbb = 0;
     for (int rank = 0; rank < kKeys; ++rank) {
       const int k = sp.key_by_rank[rank];
       if (k < 0) break;
@@ -134,14 +138,13 @@ __global__ void __launch_bounds__(kSegThreads) tb_segment_kernel(const nrldpc_tb
       const int pairs = (cnt + 1) / 2, Gk = sp.key_G[k];
       const int items = (pairs + Gk - 1) / Gk;
       s_item_base[k] = ib;
-      s_slot_base[k] = sb;
+      s_cb_base[k] = cbb;
       s_items[k] = items;
       ib += items;
-      sb += items * 2 * Gk;
+      cbb += cnt;
     }
     s_num_items = ib;
-    s_num_slots = sb;
-    if (ib > sp.max_items || sb > sp.max_slots) s_err = 1;
+    if (ib > sp.max_items) s_err = 1;
   }
   __syncthreads();
   if (s_err) {
@@ -152,19 +155,19 @@ __global__ void __launch_bounds__(kSegThreads) tb_segment_kernel(const nrldpc_tb
     }
     return;
   }
-  for (int i = tid; i < s_num_slots; i += kSegThreads) sp.slots[i] = -1;
-  __syncthreads();
-  // 4. scatter code blocks into pair slots (order inside a bucket is free:
-  //    a block's result does not depend on its lane partner)
+  if (tid < kKeys) {
+    sp.key_base[tid] = s_count[tid] ? s_cb_base[tid] : 0;
+    sp.key_count[tid] = s_count[tid];
+    sp.key_cursor[tid] = 0;
+  }
+  // 4. scatter code blocks into their graph's queue (order inside a queue is
+  //    free: a block's result does not depend on its lane partner)
   for (int c = tid; c < total; c += kSegThreads) {
     const int k = sp.cb_key[c];
     const int pos = atomicAdd(&s_cursor[k], 1);
-    const int pair = pos >> 1, Gk = sp.key_G[k];
-    const int it = pair / Gk, g = pair - it * Gk;
-    sp.slots[s_slot_base[k] + it * 2 * Gk + 2 * g + (pos & 1)] = c;
+    sp.cb_list[s_cb_base[k] + pos] = c;
   }
-  __syncthreads();
-  // 5. item records
+  // 5. item records: a claim on graph k's queue
   for (int i = tid; i < s_num_items; i += kSegThreads) {
     int k = -1;
     for (int rank = 0; rank < kKeys; ++rank) {
@@ -175,18 +178,9 @@ __global__ void __launch_bounds__(kSegThreads) tb_segment_kernel(const nrldpc_tb
         break;
       }
     }
-    const int j = i - s_item_base[k], Gk = sp.key_G[k];
-    const int pairs = (s_count[k] + 1) / 2;
     MixedItem m;
     m.graph = k;
-    m.slot_base = s_slot_base[k] + j * 2 * Gk;
-    m.npairs = min(Gk, pairs - j * Gk);
-    int bmax = 0;
-    for (int q = 0; q < 2 * m.npairs; ++q) {
-      const int c = sp.slots[m.slot_base + q];
-      if (c >= 0) bmax = max(bmax, sp.cws[c].B);
-    }
-    m.bmax_pad = (bmax + 31) & ~31;
+    m.pad0 = m.pad1 = m.pad2 = 0;
     sp.items[i] = m;
   }
   if (tid == 0) {
@@ -305,7 +299,7 @@ struct TbLane {
   int32_t* d_tb_first = nullptr;
   int32_t* d_tb_err = nullptr;
   MixedItem* d_items = nullptr;
-  int32_t* d_slots = nullptr;
+  int32_t* d_queue = nullptr;       // cb_list [max_cbs], key_base, key_count, key_cursor [kKeys each]
   int32_t* d_num_items = nullptr;   // [2]
   int32_t* d_counter = nullptr;
   uint8_t* d_cb_bits = nullptr;
@@ -319,7 +313,7 @@ struct TbLane {
 
 struct TbEngine {
   int device = 0, num_sms = 0;
-  int max_tbs = 0, max_cbs = 0, max_items = 0, max_slots = 0;
+  int max_tbs = 0, max_cbs = 0, max_items = 0;
   bool degen = false;
   int grid = 1;
   MixedGraph* d_graphs = nullptr;
@@ -359,7 +353,7 @@ void lane_free(TbLane* l) {
   cudaFree(l->d_tb_first);
   cudaFree(l->d_tb_err);
   cudaFree(l->d_items);
-  cudaFree(l->d_slots);
+  cudaFree(l->d_queue);
   cudaFree(l->d_num_items);
   cudaFree(l->d_counter);
   cudaFree(l->d_cb_bits);
@@ -386,7 +380,7 @@ int engine_lanes(TbEngine* e, int n) {
         cudaMalloc(&l->d_tb_first, (size_t)max_tbs * sizeof(int32_t)) == cudaSuccess &&
         cudaMalloc(&l->d_tb_err, (size_t)max_tbs * sizeof(int32_t)) == cudaSuccess &&
         cudaMalloc(&l->d_items, (size_t)e->max_items * sizeof(MixedItem)) == cudaSuccess &&
-        cudaMalloc(&l->d_slots, (size_t)e->max_slots * sizeof(int32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_queue, ((size_t)max_cbs + 3 * kKeys) * sizeof(int32_t)) == cudaSuccess &&
         cudaMalloc(&l->d_num_items, 2 * sizeof(int32_t)) == cudaSuccess &&
         cudaMalloc(&l->d_counter, sizeof(int32_t)) == cudaSuccess &&
         cudaMalloc(&l->d_cb_bits, (size_t)max_cbs * kCbBitsStride) == cudaSuccess &&
@@ -405,13 +399,19 @@ int engine_lanes(TbEngine* e, int n) {
     sp.tb_first = l->d_tb_first;
     sp.tb_err = l->d_tb_err;
     sp.items = l->d_items;
-    sp.slots = l->d_slots;
+    sp.cb_list = l->d_queue;
+    sp.key_base = l->d_queue + max_cbs;
+    sp.key_count = l->d_queue + max_cbs + kKeys;
+    sp.key_cursor = l->d_queue + max_cbs + 2 * kKeys;
     sp.num_items = l->d_num_items;
     sp.counter = l->d_counter;
     MixedParams& p = l->mp;
     p = e->mp;
     p.items = l->d_items;
-    p.slots = l->d_slots;
+    p.cb_list = sp.cb_list;
+    p.key_base = sp.key_base;
+    p.key_count = sp.key_count;
+    p.key_cursor = sp.key_cursor;
     p.cws = l->d_cws;
     p.num_items_dev = l->d_num_items;
     p.counter = l->d_counter;
@@ -524,7 +524,6 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
   memset(graphs.data(), 0, graphs.size() * sizeof(MixedGraph));
   std::vector<std::pair<long, int>> order;
   const int base[8] = {2, 3, 5, 7, 9, 11, 13, 15};
-  int sumG = 0;
   for (int bgn = 1; bgn <= 2; ++bgn)
     for (int s = 0; s < 8; ++s)
       for (int j = 0; (base[s] << j) <= 384; ++j) {
@@ -532,13 +531,11 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
         const int key = tb_graph_key(bgn, Zc, s);
         graphs[key] = tb_make_graph(bgn, Zc, s);
         e->sp.key_G[key] = graphs[key].G;
-        sumG += graphs[key].G;
         order.push_back(std::make_pair(-(long)base_graph(bgn).nnz * Zc, key));
       }
   std::sort(order.begin(), order.end());
   for (int r = 0; r < kKeys; ++r) e->sp.key_by_rank[r] = r < (int)order.size() ? (int16_t)order[r].second : -1;
   e->max_items = max_cbs + (int)order.size();
-  e->max_slots = 2 * max_cbs + 2 * sumG;
   int occ = occupancy_mixed(e->degen);
   if (occ < 1) occ = 1;
   e->grid = std::max(1, std::min(2, occ) * e->num_sms);
@@ -553,7 +550,6 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
   SegParams& sp = e->sp;
   sp.max_cbs = max_cbs;
   sp.max_items = e->max_items;
-  sp.max_slots = e->max_slots;
   MixedParams& p = e->mp;
   p.graphs = e->d_graphs;
   p.num_items = 0;

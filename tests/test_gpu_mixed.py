@@ -11,8 +11,8 @@ from oracle.oracle import dec_cfg, in_config, make_llrs
 pytestmark = pytest.mark.gpu
 
 
-def _build(oracle, n, seed, noise_db):
-    cfgs = random_mixed_configs(n, seed=seed)
+def _build(oracle, n, seed, noise_db, cfgs=None):
+    cfgs = cfgs or random_mixed_configs(n, seed=seed)
     llrs = []
     for i, c in enumerate(cfgs):
         llr, _ = make_llrs(oracle, in_config(*c, 0), 1, noise_db=noise_db - 0.5 * (i % 4), seed=seed * 7919 + i)
@@ -46,4 +46,37 @@ def test_mixed_batch_bit_exact_per_block(oracle, cuda, row):
     bits3, status3, _ = plan.decode(arena, use_graph=False)
     torch.cuda.synchronize()
     assert torch.equal(bits3, bits) and torch.equal(status3, status)
+    plan.close()
+
+
+def test_mixed_lane_refill_bit_exact(oracle, cuda):
+    """Many blocks of one lifting size per base graph (Zc = 16: 24 lane pairs per
+    CTA, so each graph's queue refills every finished half lane several times),
+    blocks converging at different iterations, and algo 2's iteration-dependent
+    table: every block must still decode exactly as it does alone."""
+    import ctypes
+
+    from deeplearning_5g_ldpc_decoder_b200 import capi
+
+    lib = capi.load_library()
+    pool = random_mixed_configs(16000, seed=11, rvs=(0,))
+    cfgs = []
+    for c in pool:
+        out = capi.LdpcConfig()
+        assert lib.gen_ldpc_parameters(ctypes.byref(out), ctypes.byref(capi.make_in_config(*c, 0))) == 0
+        if out.Zc == 16:
+            cfgs.append(c)
+    assert len(cfgs) >= 250
+    cfgs, llrs = _build(oracle, len(cfgs), seed=5, noise_db=-10.0, cfgs=cfgs)
+    row = [2, 9, 22936, 0, 1280, 32767, -32767]
+    plan = MixedPlan(cfgs, row)
+    arena = plan.pack_llrs(llrs)
+    bits, status, iters = plan.decode(arena, use_graph=False)
+    torch.cuda.synchronize()
+    st, it, b = status.cpu().numpy(), iters.cpu().numpy(), bits.cpu().numpy()
+    for i, c in enumerate(cfgs):
+        es, eb, ei, _ = oracle.decode(llrs[i].numpy(), in_config(*c, 0), dec_cfg(row))
+        assert (st[i], it[i]) == (es, ei), (i, c)
+        assert np.array_equal(b[plan.bits_offsets[i]: plan.bits_offsets[i] + plan.nbytes[i]], eb), (i, c)
+    assert len(set(it.tolist())) >= 5      # blocks finish at many different iterations
     plan.close()
