@@ -131,12 +131,14 @@ struct DeviceState {
   // host-buffer batched API
   struct HostStage {
     Buffer llr, bits, stat, iters;
-    cudaStream_t copy = nullptr, comp = nullptr;   // copy engine / decode streams of the pipeline
+    cudaStream_t copy = nullptr;                   // copy-engine stream of the pipeline
+    cudaStream_t comp[2] = {nullptr, nullptr};     // decode streams: chunks alternate between them
     cudaEvent_t start = nullptr;
     std::vector<cudaEvent_t> h2d, dec;             // per chunk
   };
   std::map<cudaStream_t, HostStage> host_stage;
   std::map<cudaStream_t, Buffer> scratch;
+  std::map<cudaStream_t, Buffer> queue;   // fixed point: code-block queue head + finished-CTA count
   int num_sms = 0;
 };
 
@@ -275,7 +277,7 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
 
   int occ;
   if (fixed) {
-    occ = occupancy_fixed(plan->block, plan->smem, plan->degen);
+    occ = occupancy_fixed(plan->block, plan->smem, plan->degen, true);
   } else if (algo == 4) {
     occ = occupancy_float_minsum(plan->block, plan->smem);
   } else {
@@ -334,6 +336,15 @@ int32_t decode_batch_locked(const int16_t* d_llr, int64_t llr_stride, int32_t nu
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (scratch_for(st, s, plan.scratch_bytes, &scratch) != 0) return NRLDPC_ERR_CUDA;
   DecodeParams& p = plan.p;
+  if (dc->algo >= 1 && dc->algo <= 3 && p.num_items > plan.grid) {
+    // More than one wave: half lanes refill from the stream's code-block queue
+    // (zeroed once, rewound by each launch's last CTA).  Within one wave there
+    // is nothing to refill from, and the fixed work items are a little faster.
+    Buffer& q = st->queue[s];
+    if (!q.ptr && (ensure(&q, 256) != 0 || cudaMemsetAsync(q.ptr, 0, 256, s) != cudaSuccess))
+      return NRLDPC_ERR_CUDA;
+    p.cursor = static_cast<int32_t*>(q.ptr);
+  }
   p.llr = d_llr;
   p.llr_stride = llr_stride;
   p.bits = d_bits;
@@ -687,13 +698,16 @@ int32_t nrldpc_decode_batch_host(const int16_t* h_llr, int64_t llr_stride, int32
     return NRLDPC_ERR_CUDA;
   if (!hs.copy) {
     if (cudaStreamCreateWithFlags(&hs.copy, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&hs.comp, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&hs.comp[0], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&hs.comp[1], cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&hs.start, cudaEventDisableTiming) != cudaSuccess)
       return NRLDPC_ERR_CUDA;
   }
   // Chunks of whole waves of the decode kernel: chunk k+1's host-to-device copy
   // overlaps chunk k's decode, and the waves of the chunks add up to the waves of
   // one launch over the whole batch, so nothing is lost to partial waves.
+  // Consecutive chunks decode on two streams, so the CTAs of chunk k+1 start on
+  // the SMs that chunk k's first finishers leave free (no tail per chunk).
   Plan probe;
   if (make_plan(cp, *decoder_cfg, num_cw, st, &probe) != 0) return NRLDPC_ERR_CUDA;
   const bool fixed = decoder_cfg->algo >= 1 && decoder_cfg->algo <= 3;
@@ -717,7 +731,8 @@ int32_t nrldpc_decode_batch_host(const int16_t* h_llr, int64_t llr_stride, int32
   }
   // work already queued on the caller's stream comes first
   if (cudaEventRecord(hs.start, s) != cudaSuccess || cudaStreamWaitEvent(hs.copy, hs.start, 0) != cudaSuccess ||
-      cudaStreamWaitEvent(hs.comp, hs.start, 0) != cudaSuccess)
+      cudaStreamWaitEvent(hs.comp[0], hs.start, 0) != cudaSuccess ||
+      cudaStreamWaitEvent(hs.comp[1], hs.start, 0) != cudaSuccess)
     return NRLDPC_ERR_CUDA;
   int16_t* d_llr = static_cast<int16_t*>(hs.llr.ptr);
   uint8_t* d_bits = static_cast<uint8_t*>(hs.bits.ptr);
@@ -733,12 +748,13 @@ int32_t nrldpc_decode_batch_host(const int16_t* h_llr, int64_t llr_stride, int32
   }
   for (int k = 0; k < nchunks; ++k) {
     const int64_t c0 = k * chunk, n = std::min<int64_t>(chunk, num_cw - c0);
-    if (cudaStreamWaitEvent(hs.comp, hs.h2d[k], 0) != cudaSuccess) return NRLDPC_ERR_CUDA;
+    cudaStream_t comp = hs.comp[k & 1];
+    if (cudaStreamWaitEvent(comp, hs.h2d[k], 0) != cudaSuccess) return NRLDPC_ERR_CUDA;
     const int32_t rc = decode_batch_locked(d_llr + (size_t)c0 * (size_t)llr_stride, llr_stride, (int32_t)n, inconfig,
                                            decoder_cfg, d_bits + (size_t)c0 * (size_t)bits_stride, bits_stride,
-                                           d_stat + c0, d_iters + c0, nullptr, 0, nullptr, 0, hs.comp);
+                                           d_stat + c0, d_iters + c0, nullptr, 0, nullptr, 0, comp);
     if (rc != NRLDPC_OK) return rc;
-    if (cudaEventRecord(hs.dec[k], hs.comp) != cudaSuccess || cudaStreamWaitEvent(hs.copy, hs.dec[k], 0) != cudaSuccess)
+    if (cudaEventRecord(hs.dec[k], comp) != cudaSuccess || cudaStreamWaitEvent(hs.copy, hs.dec[k], 0) != cudaSuccess)
       return NRLDPC_ERR_CUDA;
     if (decoder_cfg->max_iterations > 0 &&
         cudaMemcpyAsync(h_hardbits + (size_t)c0 * (size_t)bits_stride, d_bits + (size_t)c0 * (size_t)bits_stride,

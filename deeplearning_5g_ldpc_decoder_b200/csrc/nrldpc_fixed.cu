@@ -21,13 +21,18 @@
 //    pair (two scaled minima, the position of the minimum, one sign bit per
 //    edge: 16 or 20 bytes for both code blocks instead of 4*degree) in a
 //    per-CTA global scratch that stays resident in L2.
-//  * The grid is persistent: each CTA loops over work items of G pairs.
+//  * The grid is persistent.  With a block cursor (DecodeParams::cursor: the
+//    queue head and a count of finished CTAs, both zero at launch and rewound
+//    by the last CTA to finish) every int16 half lane takes code blocks from one
+//    device queue: as soon as its block passes the CRC or reaches
+//    max_iterations the block's outputs are written and the half lane
+//    restarts on the next block (zero messages through the `fresh` mask, its
+//    own iteration count), so each block costs its own iterations.  Without a
+//    cursor (the no-allocation entry point) each CTA loops over fixed work
+//    items of G pairs until every block of the item has finished.
 //  * CRC early termination runs every iteration inside the kernel: each hard
 //    bit i contributes x^(B-1-i+W) mod g(x) (a precomputed table), the
 //    contributions are XOR-reduced with warp reductions and shared atomics.
-//    A code block that passes stops being reported (its outputs are written at
-//    that iteration); the CTA leaves the iteration loop once every code block
-//    in it has passed.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -70,7 +75,81 @@ __device__ void emit_block(const DecodeParams& p, const uint32_t* lq, int zx, in
   }
 }
 
-template <bool kDegenClip>
+// Hard decisions + CRC remainder of both halves of every group into s_crc
+// (zero for a block whose CRC passes).  Warp-uniform trip count: Bp and the
+// block size are multiples of 32.
+__device__ __forceinline__ void crc_pass(const DecodeParams& p, const uint32_t* s_lq, uint32_t* s_crc, int Bp) {
+  for (int k = threadIdx.x; k < p.G * Bp; k += blockDim.x) {
+    const int gg = k / Bp;
+    const int i = k - gg * Bp;
+    uint32_t r0 = 0u, r1 = 0u;
+    if (i < p.B) {
+      const uint32_t w = s_lq[gg * p.lq_len + i];
+      const uint32_t tv = crc_term(p, i);
+      r0 = (w & 0x8000u) ? tv : 0u;
+      r1 = (w & 0x80000000u) ? tv : 0u;
+    }
+    r0 = __reduce_xor_sync(0xFFFFFFFFu, r0);
+    r1 = __reduce_xor_sync(0xFFFFFFFFu, r1);
+    if ((threadIdx.x & 31) == 0) {
+      if (r0) atomicXor(&s_crc[2 * gg], r0);
+      if (r1) atomicXor(&s_crc[2 * gg + 1], r1);
+    }
+  }
+}
+
+// Rate recovery into the halves of the group's LQ words selected by r0 / r1
+// (half h gets code block cw_h, zeros when cw_h < 0), with the soft buffers;
+// the other half keeps its bits.  One pass for both halves.
+__device__ __forceinline__ void recover_halves(const DecodeParams& p, uint32_t* lq, int zx, int cw0, int cw1,
+                                               bool r0, bool r1) {
+  const uint32_t keep = (r0 ? 0u : 0x0000FFFFu) | (r1 ? 0u : 0xFFFF0000u);
+  const bool v0 = r0 && cw0 >= 0, v1 = r1 && cw1 >= 0;
+  const int16_t* in0 = p.llr + (int64_t)(v0 ? cw0 : 0) * p.llr_stride;
+  const int16_t* in1 = p.llr + (int64_t)(v1 ? cw1 : 0) * p.llr_stride;
+  int16_t* h0 = (p.harq && v0) ? p.harq + (int64_t)cw0 * p.harq_stride : nullptr;
+  int16_t* h1 = (p.harq && v1) ? p.harq + (int64_t)cw1 * p.harq_stride : nullptr;
+  for (int i = zx; i < p.lq_len; i += p.Zc) {
+    uint32_t w = keep ? (lq[i] & keep) : 0u;
+    if (v0) {
+      const int32_t a = recover_position(p, in0, i, (p.harq_on && h0) ? h0[i] : 0);
+      if (h0) h0[i] = (int16_t)a;
+      w |= (uint32_t)a & 0xFFFFu;
+    }
+    if (v1) {
+      const int32_t a = recover_position(p, in1, i, (p.harq_on && h1) ? h1[i] : 0);
+      if (h1) h1[i] = (int16_t)a;
+      w |= (uint32_t)a << 16;
+    }
+    lq[i] = w;
+  }
+}
+
+// Next code blocks of the queue for the half lanes that ask (q0 / q1: this
+// thread asks for half 0 / half 1), one atomic per warp.  Called by whole
+// warps; returns -1 past the end of the queue.
+__device__ __forceinline__ void take_blocks(const DecodeParams& p, bool q0, bool q1, int* cw0, int* cw1) {
+  const unsigned b0 = __ballot_sync(0xFFFFFFFFu, q0);
+  const unsigned b1 = __ballot_sync(0xFFFFFFFFu, q1);
+  const int n0 = __popc(b0), total = n0 + __popc(b1);
+  if (total == 0) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(b0 | b1) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(p.cursor, total);
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  const unsigned lt = (1u << lane) - 1u;
+  if (q0) {
+    const int i = base + __popc(b0 & lt);
+    *cw0 = i < p.num_cw ? i : -1;
+  }
+  if (q1) {
+    const int i = base + n0 + __popc(b1 & lt);
+    *cw1 = i < p.num_cw ? i : -1;
+  }
+}
+
+template <bool kDegenClip, bool kRefill>
 __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __grid_constant__ DecodeParams p) {
   extern __shared__ __align__(16) uint32_t s_lq[];        // [G][lq_len] int16x2
   __shared__ uint32_t s_crc[2 * kMaxGroups];
@@ -88,124 +167,197 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
   const uint32_t zxm4 = zx4 - 4u * (uint32_t)p.Zc;     // wraps: min(zx4+s, zxm4+s) = ((zx+V) mod Zc)*4
   const uint32_t gb4 = 4u * (uint32_t)((active ? g : 0) * p.lq_len);
 
-  for (int item = blockIdx.x; item < p.num_items; item += gridDim.x) {
-    const int pair = item * p.G + g;
-    const int cw0 = 2 * pair, cw1 = 2 * pair + 1;
-    const bool v0 = active && cw0 < p.num_cw;
-    const bool v1 = active && cw1 < p.num_cw;
-
-    // ---- rate recovery into LQ (and the soft buffers) ----
-    if (active) {
-      const int16_t* in0 = p.llr + (int64_t)(v0 ? cw0 : 0) * p.llr_stride;
-      const int16_t* in1 = p.llr + (int64_t)(v1 ? cw1 : 0) * p.llr_stride;
-      int16_t* h0 = (p.harq && v0) ? p.harq + (int64_t)cw0 * p.harq_stride : nullptr;
-      int16_t* h1 = (p.harq && v1) ? p.harq + (int64_t)cw1 * p.harq_stride : nullptr;
-      for (int i = zx; i < p.lq_len; i += p.Zc) {
-        int32_t a0 = 0, a1 = 0;
-        if (p.harq_on) {
-          if (h0) a0 = h0[i];
-          if (h1) a1 = h1[i];
-        }
-        a0 = v0 ? recover_position(p, in0, i, a0) : 0;
-        a1 = v1 ? recover_position(p, in1, i, a1) : 0;
-        if (h0) h0[i] = (int16_t)a0;
-        if (h1) h1[i] = (int16_t)a1;
-        lq[i] = ((uint32_t)a0 & 0xFFFFu) | ((uint32_t)a1 << 16);
-      }
-    }
-    if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
-    // Padding slots count as finished so they never hold the CTA back.
-    bool done0 = !v0, done1 = !v1;
+  if constexpr (kRefill) {
+    __shared__ int s_cw[2 * kMaxGroups];   // block in each half lane, -1 when idle
+    __shared__ int s_base;
+    if (tid == 0) s_base = atomicAdd(p.cursor, 2 * p.G);
     __syncthreads();
-
-    int it = 0;
-    for (; it < p.max_it; ++it) {
-      for (int row = 0; row < p.R; ++row) {
+    int cw[2] = {-1, -1};
+    if (active) {
+      cw[0] = s_base + 2 * g < p.num_cw ? s_base + 2 * g : -1;
+      cw[1] = s_base + 2 * g + 1 < p.num_cw ? s_base + 2 * g + 1 : -1;
+      recover_halves(p, lq, zx, cw[0], cw[1], true, true);
+    }
+    int itv[2] = {0, 0};
+    if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
+    uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
+    bool idle = __syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0));
+    const bool run = p.max_it > 0;   // max_iterations == 0: rate recovery only, status 1
+    while (!idle) {
+      for (int row = 0; run && row < p.R; ++row) {
         if (active) {
           const int e0 = p.row_off[row];
           const int deg = p.row_off[row + 1] - e0;
-          const uint32_t ab = p.weights_T > 0 ? __ldg(p.weights + (min(it, p.weights_T - 1) * p.R + row))
-                                              : p.w_inline[row];
-          const int32_t alpha = (int32_t)(int16_t)(ab & 0xFFFFu);
-          const int32_t beta = ((int32_t)ab) >> 16;
-          layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0, alpha, beta,
-                                           alpha, beta, it == 0 ? 0xFFFFFFFFu : 0u, scratch + p.lr_off[row] + tid);
+          uint32_t ab0, ab1;
+          if (p.weights_T > 0) {
+            ab0 = __ldg(p.weights + (min(itv[0], p.weights_T - 1) * p.R + row));
+            ab1 = __ldg(p.weights + (min(itv[1], p.weights_T - 1) * p.R + row));
+          } else {
+            ab0 = ab1 = p.w_inline[row];
+          }
+          layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0,
+                                           (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
+                                           (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, fresh,
+                                           scratch + p.lr_off[row] + tid);
         }
         __syncthreads();
       }
-
-      // ---- hard decisions + CRC of every code block in the CTA ----
-      for (int k = tid; k < p.G * Bp; k += blockDim.x) {
-        const int gg = k / Bp;          // warp-uniform: Bp and blockDim are multiples of 32
-        const int i = k - gg * Bp;
-        uint32_t r0 = 0u, r1 = 0u;
-        if (i < p.B) {
-          const uint32_t w = s_lq[gg * p.lq_len + i];
-          const uint32_t tv = crc_term(p, i);
-          r0 = (w & 0x8000u) ? tv : 0u;
-          r1 = (w & 0x80000000u) ? tv : 0u;
+      fresh = 0u;
+      if (run) crc_pass(p, s_lq, s_crc, Bp);
+      __syncthreads();
+      bool fin[2] = {false, false};
+      if (active) {
+        for (int h = 0; h < 2; ++h) {
+          if (cw[h] < 0) continue;
+          if (run) ++itv[h];
+          const bool pass = run && s_crc[2 * g + h] == 0u;
+          if (pass || itv[h] >= p.max_it) {
+            emit_block(p, lq, zx, cw[h], h, pass ? 0 : 1, itv[h]);
+            fin[h] = true;
+          }
         }
-        r0 = __reduce_xor_sync(0xFFFFFFFFu, r0);
-        r1 = __reduce_xor_sync(0xFFFFFFFFu, r1);
-        if ((tid & 31) == 0) {
-          if (r0) atomicXor(&s_crc[2 * gg], r0);
-          if (r1) atomicXor(&s_crc[2 * gg + 1], r1);
-        }
+      }
+      // s_crc read and the finished blocks emitted before anything is reused
+      const bool any = __syncthreads_or(fin[0] || fin[1]);
+      if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
+      if (!any) continue;
+      int nc0 = -1, nc1 = -1;
+      take_blocks(p, fin[0] && zx == 0, fin[1] && zx == 0, &nc0, &nc1);
+      if (zx == 0) {
+        if (fin[0]) s_cw[2 * g] = nc0;
+        if (fin[1]) s_cw[2 * g + 1] = nc1;
       }
       __syncthreads();
-      bool pass0 = false, pass1 = false;
+      if (active && (fin[0] || fin[1])) {
+        for (int h = 0; h < 2; ++h) {
+          if (!fin[h]) continue;
+          cw[h] = s_cw[2 * g + h];
+          itv[h] = 0;
+          if (cw[h] >= 0) fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
+        }
+        recover_halves(p, lq, zx, cw[0], cw[1], fin[0], fin[1]);
+      }
+      idle = __syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0));
+    }
+    // Every take of this CTA is done (the last barrier above).  The CTA that
+    // finishes last rewinds the queue for the next launch on the stream.
+    if (tid == 0) {
+      __threadfence();
+      if (atomicAdd(p.cursor + 1, 1) == (int)gridDim.x - 1) {
+        atomicExch(p.cursor, 0);
+        atomicExch(p.cursor + 1, 0);
+      }
+    }
+  } else {
+    for (int item = blockIdx.x; item < p.num_items; item += gridDim.x) {
+      const int pair = item * p.G + g;
+      const int cw0 = 2 * pair, cw1 = 2 * pair + 1;
+      const bool v0 = active && cw0 < p.num_cw;
+      const bool v1 = active && cw1 < p.num_cw;
+
+      // ---- rate recovery into LQ (and the soft buffers) ----
       if (active) {
-        pass0 = !done0 && s_crc[2 * g] == 0u;
-        pass1 = !done1 && s_crc[2 * g + 1] == 0u;
-        if (pass0) emit_block(p, lq, zx, cw0, 0, 0, it + 1);
-        if (pass1) emit_block(p, lq, zx, cw1, 1, 0, it + 1);
-        done0 = done0 || pass0;
-        done1 = done1 || pass1;
+        const int16_t* in0 = p.llr + (int64_t)(v0 ? cw0 : 0) * p.llr_stride;
+        const int16_t* in1 = p.llr + (int64_t)(v1 ? cw1 : 0) * p.llr_stride;
+        int16_t* h0 = (p.harq && v0) ? p.harq + (int64_t)cw0 * p.harq_stride : nullptr;
+        int16_t* h1 = (p.harq && v1) ? p.harq + (int64_t)cw1 * p.harq_stride : nullptr;
+        for (int i = zx; i < p.lq_len; i += p.Zc) {
+          int32_t a0 = 0, a1 = 0;
+          if (p.harq_on) {
+            if (h0) a0 = h0[i];
+            if (h1) a1 = h1[i];
+          }
+          a0 = v0 ? recover_position(p, in0, i, a0) : 0;
+          a1 = v1 ? recover_position(p, in1, i, a1) : 0;
+          if (h0) h0[i] = (int16_t)a0;
+          if (h1) h1[i] = (int16_t)a1;
+          lq[i] = ((uint32_t)a0 & 0xFFFFu) | ((uint32_t)a1 << 16);
+        }
       }
-      // Everyone has read s_crc before it is cleared for the next iteration.
-      const bool all_done = __syncthreads_and(done0 && done1);
       if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
-      if (all_done) {
-        ++it;
-        break;
+      // Padding slots count as finished so they never hold the CTA back.
+      bool done0 = !v0, done1 = !v1;
+      __syncthreads();
+
+      int it = 0;
+      for (; it < p.max_it; ++it) {
+        for (int row = 0; row < p.R; ++row) {
+          if (active) {
+            const int e0 = p.row_off[row];
+            const int deg = p.row_off[row + 1] - e0;
+            const uint32_t ab = p.weights_T > 0 ? __ldg(p.weights + (min(it, p.weights_T - 1) * p.R + row))
+                                                : p.w_inline[row];
+            const int32_t alpha = (int32_t)(int16_t)(ab & 0xFFFFu);
+            const int32_t beta = ((int32_t)ab) >> 16;
+            layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0, alpha, beta,
+                                             alpha, beta, it == 0 ? 0xFFFFFFFFu : 0u, scratch + p.lr_off[row] + tid);
+          }
+          __syncthreads();
+        }
+
+        // ---- hard decisions + CRC of every code block in the CTA ----
+        crc_pass(p, s_lq, s_crc, Bp);
+        __syncthreads();
+        bool pass0 = false, pass1 = false;
+        if (active) {
+          pass0 = !done0 && s_crc[2 * g] == 0u;
+          pass1 = !done1 && s_crc[2 * g + 1] == 0u;
+          if (pass0) emit_block(p, lq, zx, cw0, 0, 0, it + 1);
+          if (pass1) emit_block(p, lq, zx, cw1, 1, 0, it + 1);
+          done0 = done0 || pass0;
+          done1 = done1 || pass1;
+        }
+        // Everyone has read s_crc before it is cleared for the next iteration.
+        const bool all_done = __syncthreads_and(done0 && done1);
+        if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
+        if (all_done) {
+          ++it;
+          break;
+        }
       }
+      if (active) {
+        if (!done0) emit_block(p, lq, zx, cw0, 0, 1, it);
+        if (!done1) emit_block(p, lq, zx, cw1, 1, 1, it);
+      }
+      __syncthreads();   // LQ and s_crc are reused by the next work item
     }
-    if (active) {
-      if (!done0) emit_block(p, lq, zx, cw0, 0, 1, it);
-      if (!done1) emit_block(p, lq, zx, cw1, 1, 1, it);
-    }
-    __syncthreads();   // LQ and s_crc are reused by the next work item
   }
+}
+
+template <bool kDegenClip, bool kRefill>
+int launch_fixed_t(const DecodeParams& p, int grid, int block, int smem, cudaStream_t s) {
+  const cudaError_t err =
+      cudaFuncSetAttribute(fixed_pair_kernel<kDegenClip, kRefill>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (err != cudaSuccess) return (int)err;
+  fixed_pair_kernel<kDegenClip, kRefill><<<grid, block, smem, s>>>(p);
+  return (int)cudaSuccess;
+}
+
+template <bool kDegenClip, bool kRefill>
+int occupancy_fixed_t(int block, int smem) {
+  int n = 0;
+  cudaFuncSetAttribute(fixed_pair_kernel<kDegenClip, kRefill>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_pair_kernel<kDegenClip, kRefill>, block, smem);
+  return n;
 }
 
 }  // namespace
 
 int launch_fixed(const DecodeParams& p, int grid, int block, int smem, bool degen_clip, void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  cudaError_t err;
-  if (degen_clip) {
-    err = cudaFuncSetAttribute(fixed_pair_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (err != cudaSuccess) return (int)err;
-    fixed_pair_kernel<true><<<grid, block, smem, s>>>(p);
-  } else {
-    err = cudaFuncSetAttribute(fixed_pair_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (err != cudaSuccess) return (int)err;
-    fixed_pair_kernel<false><<<grid, block, smem, s>>>(p);
-  }
+  const bool refill = p.cursor != nullptr;
+  const int err = degen_clip ? (refill ? launch_fixed_t<true, true>(p, grid, block, smem, s)
+                                       : launch_fixed_t<true, false>(p, grid, block, smem, s))
+                             : (refill ? launch_fixed_t<false, true>(p, grid, block, smem, s)
+                                       : launch_fixed_t<false, false>(p, grid, block, smem, s));
+  if (err != (int)cudaSuccess) return err;
   count_launch();
   return (int)cudaGetLastError();
 }
 
-int occupancy_fixed(int block, int smem, bool degen_clip) {
-  int n = 0;
-  if (degen_clip) {
-    cudaFuncSetAttribute(fixed_pair_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_pair_kernel<true>, block, smem);
-  } else {
-    cudaFuncSetAttribute(fixed_pair_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_pair_kernel<false>, block, smem);
-  }
-  return n;
+int occupancy_fixed(int block, int smem, bool degen_clip, bool refill) {
+  if (degen_clip) return refill ? occupancy_fixed_t<true, true>(block, smem) : occupancy_fixed_t<true, false>(block, smem);
+  return refill ? occupancy_fixed_t<false, true>(block, smem) : occupancy_fixed_t<false, false>(block, smem);
 }
 
 }  // namespace nrldpc

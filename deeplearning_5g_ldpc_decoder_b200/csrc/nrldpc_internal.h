@@ -86,6 +86,8 @@ struct DecodeParams {
   int64_t harq_stride;
   uint32_t* scratch;
   int64_t scratch_words;   // per CTA
+  int32_t* cursor;         // fixed point: [queue head, finished CTAs], zero at launch, rewound by the
+                           // kernel's last CTA (null: fixed work items)
   // Per edge: (base column * Zc) in the low 16 bits, (V_ij mod Zc) in the high.
   uint32_t edge[kMaxNnz];
   // The same two fields as byte offsets of 32-bit shared-memory words
@@ -201,7 +203,7 @@ int launch_float_minsum(const DecodeParams& p, int grid, int block, int smem, vo
 int launch_float_bp(const DecodeParams& p, int grid, int block, int smem, void* stream);
 
 // Occupancy helpers (per kernel variant).
-int occupancy_fixed(int block, int smem, bool degen_clip);
+int occupancy_fixed(int block, int smem, bool degen_clip, bool refill = false);
 int occupancy_float_minsum(int block, int smem);
 int occupancy_float_bp(int block, int smem);
 
