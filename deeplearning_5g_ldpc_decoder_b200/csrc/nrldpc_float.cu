@@ -122,20 +122,25 @@ __device__ __forceinline__ float bp_message(float prod) {
   return __fmul_rn(2.0f, atanhf(prod));
 }
 
+// Registers are what limits this kernel's occupancy, so the row keeps only
+// tanh values and suffix products live: rel = LQ - old message is parked in
+// LQ's own shared-memory word until the update (a row's edges are distinct
+// words that no other thread touches during the layer), edge addresses are
+// recomputed from the constant-cache table, and the prefix product runs as a
+// scalar.  The arithmetic and its order are unchanged.
 template <int D>
 __device__ __forceinline__ void bp_row(const DecodeParams& p, float* __restrict__ lq, uint32_t zx, int e0,
                                        bool first, uint32_t* __restrict__ lrp, int NT) {
-  float rel[D], th[D];
-  uint32_t addr[D];
+  float th[D];
   int nz = 0, zidx = -1;
   float nzprod = 1.0f;
   // compute_tanh_values (:65-82): tanh(rel/2), zero count, product of non-zeros.
 #pragma unroll
   for (int j = 0; j < D; ++j) {
-    addr[j] = edge_addr(p, e0 + j, zx);
+    const uint32_t a = edge_addr(p, e0 + j, zx);
     const float old = first ? 0.0f : __uint_as_float(lrp[j * NT]);
-    const float v = __fsub_rn(lq[addr[j]], old);
-    rel[j] = v;
+    const float v = __fsub_rn(lq[a], old);
+    lq[a] = v;
     if (v == 0.0f) {
       ++nz;
       zidx = j;
@@ -145,33 +150,34 @@ __device__ __forceinline__ void bp_row(const DecodeParams& p, float* __restrict_
       nzprod = __fmul_rn(nzprod, th[j]);
     }
   }
-  float msg[D];
-  if (nz == 1) {
+  if (nz == 0) {
+    // prefix/suffix products (:85-96, :135-145), same multiplication order:
+    // sf[j] = th[D-1] * ... * th[j+1] accumulated right to left (sf[D-1] = 1),
+    // the prefix th[0] * ... * th[j-1] left to right.
+    float sf[D];
+    sf[D - 1] = 1.0f;
 #pragma unroll
-    for (int j = 0; j < D; ++j) msg[j] = 0.0f;
-    const float m = bp_message(nzprod);
+    for (int j = D - 2; j >= 0; --j) sf[j] = __fmul_rn(sf[j + 1], th[j + 1]);
+    float pre = 1.0f;
 #pragma unroll
-    for (int j = 0; j < D; ++j)
-      if (j == zidx) msg[j] = m;
-  } else if (nz >= 2) {
-#pragma unroll
-    for (int j = 0; j < D; ++j) msg[j] = 0.0f;
+    for (int j = 0; j < D; ++j) {
+      const float m = bp_message(__fmul_rn(pre, sf[j]));
+      pre = __fmul_rn(pre, th[j]);
+      const uint32_t a = edge_addr(p, e0 + j, zx);
+      lrp[j * NT] = __float_as_uint(m);
+      lq[a] = __fadd_rn(lq[a], m);   // no clipping in BP (:148-150)
+    }
   } else {
-    // prefix/suffix products (:85-96, :135-145), same multiplication order.
-    float pre[D + 1], suf[D + 1];
-    pre[0] = 1.0f;
+    // one zero input: only its edge gets a message (the product of the
+    // others); two or more: every message is zero
+    const float mz = nz == 1 ? bp_message(nzprod) : 0.0f;
 #pragma unroll
-    for (int j = 0; j < D; ++j) pre[j + 1] = __fmul_rn(pre[j], th[j]);
-    suf[D] = 1.0f;
-#pragma unroll
-    for (int j = D - 1; j >= 0; --j) suf[j] = __fmul_rn(suf[j + 1], th[j]);
-#pragma unroll
-    for (int j = 0; j < D; ++j) msg[j] = bp_message(__fmul_rn(pre[j], suf[j + 1]));
-  }
-#pragma unroll
-  for (int j = 0; j < D; ++j) {
-    lrp[j * NT] = __float_as_uint(msg[j]);
-    lq[addr[j]] = __fadd_rn(rel[j], msg[j]);   // no clipping in BP (:148-150)
+    for (int j = 0; j < D; ++j) {
+      const float m = j == zidx && nz == 1 ? mz : 0.0f;
+      const uint32_t a = edge_addr(p, e0 + j, zx);
+      lrp[j * NT] = __float_as_uint(m);
+      lq[a] = __fadd_rn(lq[a], m);
+    }
   }
 }
 
@@ -215,7 +221,7 @@ __device__ void emit_float_block(const DecodeParams& p, const float* lq, int zx,
 }
 
 template <bool kBP>
-__global__ void __launch_bounds__(kThreadsTarget) float_kernel(const __grid_constant__ DecodeParams p) {
+__global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_constant__ DecodeParams p) {
   extern __shared__ __align__(16) float s_lqf[];     // [G][lq_len]
   __shared__ uint32_t s_crc[kMaxGroups];
 
