@@ -466,9 +466,10 @@ int32_t encode_one(uint8_t* infobytes, uint8_t* rm_bytes, ldpc_in_config_t* inco
   return NRLDPC_OK;
 }
 
-// Launch geometry of the training kernels for one configuration.  The float64
-// variant needs 2 (N+2Zc) doubles of shared memory per code block in the
-// backward, so it runs fewer blocks per CTA (and not at all where one does not fit).
+// Launch geometry of the training kernels for one configuration.  One code
+// block needs at least one (N+2Zc)-value array of shared memory (the backward
+// can hold LQ and dLQ in the same array at different times); the float64
+// variant runs fewer blocks per CTA.
 int make_train_params(const ldpc_in_config_t* cfg, int32_t T, int32_t batch, double clip, bool f64, TrainParams* p,
                       int* block, int* smem_fwd, int* smem_bwd) {
   CodeParams cp;
@@ -479,8 +480,8 @@ int make_train_params(const ldpc_in_config_t* cfg, int32_t T, int32_t batch, dou
   const int real = f64 ? 8 : 4;
   const int smem_cap = 227 * 1024 - 1024;   // opt-in shared memory per block, less the static reduction buffer
   int G = std::max(1, kThreadsTarget / cp.Zc);
-  while (G > 1 && 2 * G * cp.lq_len * real > smem_cap) --G;
-  if (2 * G * cp.lq_len * real > smem_cap) return NRLDPC_ERR_CONFIG;
+  while (G > 1 && G * cp.lq_len * real > smem_cap) --G;
+  if (G * cp.lq_len * real > smem_cap) return NRLDPC_ERR_CONFIG;
   p->Zc = cp.Zc;
   p->R = g.rows;
   p->n = cp.lq_len;
@@ -495,33 +496,41 @@ int make_train_params(const ldpc_in_config_t* cfg, int32_t T, int32_t batch, dou
   for (int r = 0; r <= g.rows; ++r) p->row_off[r] = g.row_off[r];
   *block = (p->G * cp.Zc + 31) & ~31;
   *smem_fwd = p->G * cp.lq_len * real;
-  *smem_bwd = 2 * p->G * cp.lq_len * real;
+  *smem_bwd = p->G * cp.lq_len * real;   // with LQ and dLQ sharing the array; pick_train_groups decides
   return NRLDPC_OK;
 }
 
 // Code blocks per CTA (G) that put the most code blocks on an SM, given the
-// kernel's registers and shared memory (one or two (N+2Zc)-value arrays per
-// block); the largest G among equals.  Returns the blocks per SM of that
-// choice and sets p->G, *block, *smem.
+// kernel's registers and shared memory (one (N+2Zc)-value array per block in
+// the forward; two in the backward, or one when LQ and dLQ share it, which the
+// backward does only where that puts more blocks on an SM, since it costs a
+// round trip of dLQ through global memory per iteration); the largest G among
+// equals.  Returns the blocks per SM of that choice and sets p->G, p->alias,
+// *block, *smem.
 int pick_train_groups(TrainParams* p, bool backward, bool f64, int* block, int* smem) {
-  const int per = (backward ? 2 : 1) * p->n * (f64 ? 8 : 4);
+  const int real = f64 ? 8 : 4;
   const int smem_cap = 227 * 1024 - 1024;
   const int gmax = std::max(1, kThreadsTarget / p->Zc);
-  int best_g = 0, best_cw = 0, best_occ = 0;
-  for (int G = gmax; G >= 1; --G) {
-    if (G * per > smem_cap) continue;
-    const int blk = (G * p->Zc + 31) & ~31;
-    const int occ = occupancy_train(backward, f64, p->R == 42, blk, G * per);
-    if (occ * G > best_cw) {
-      best_cw = occ * G;
-      best_g = G;
-      best_occ = occ;
+  int best_g = 0, best_cw = 0, best_occ = 0, best_alias = 0;
+  for (int alias = 0; alias <= (backward ? 1 : 0); ++alias) {
+    const int per = (backward && !alias ? 2 : 1) * p->n * real;
+    for (int G = gmax; G >= 1; --G) {
+      if (G * per > smem_cap) continue;
+      const int blk = (G * p->Zc + 31) & ~31;
+      const int occ = occupancy_train(backward, f64, p->R == 42, blk, G * per, alias != 0);
+      if (occ * G > best_cw) {
+        best_cw = occ * G;
+        best_g = G;
+        best_occ = occ;
+        best_alias = alias;
+      }
     }
   }
   if (best_g == 0) return 0;
   p->G = best_g;
+  p->alias = best_alias;
   *block = (best_g * p->Zc + 31) & ~31;
-  *smem = best_g * per;
+  *smem = best_g * (backward && !best_alias ? 2 : 1) * p->n * real;
   return best_occ;
 }
 

@@ -164,6 +164,7 @@ struct MixedParams {
 // ---- differentiable unrolled float min-sum (training) ----
 struct TrainParams {
   int32_t Zc, R, n, G, nnz, T, batch, detach;
+  int32_t alias;              // backward: LQ and dLQ share one shared-memory array per block
   int32_t msg_words;          // 32-bit words of compressed messages per lifted row block (4 Zc f32, 6 Zc f64)
   double clip;                // +inf when LLRs are not clipped
   // Real = float or double, per the entry point.
@@ -190,7 +191,7 @@ struct TrainParams {
 int launch_encode(const EncodeParams& p, void* stream);
 int launch_train_forward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream);
 int launch_train_backward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream);
-int occupancy_train(bool backward, bool f64, bool bg2, int block, int smem);
+int occupancy_train(bool backward, bool f64, bool bg2, int block, int smem, bool alias = false);
 int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream);
 int prepare_mixed(bool degen_clip);
 int occupancy_mixed(bool degen_clip);

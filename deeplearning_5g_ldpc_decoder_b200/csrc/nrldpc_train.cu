@@ -272,8 +272,10 @@ __global__ void __launch_bounds__(kThreadsTarget) train_forward_kernel(const __g
   }
 }
 
-template <typename Real, int kMaxD>
-__global__ void __launch_bounds__(kThreadsTarget) train_backward_kernel(const __grid_constant__ TrainParams p) {
+// Float BG2 (kMaxD 10): at most 85 registers, so two 384-thread CTAs fit an SM.
+template <typename Real, int kMaxD, bool kAlias>
+__global__ void __launch_bounds__(kThreadsTarget, (kMaxD > 10 || sizeof(Real) > 4) ? 1 : 2)
+    train_backward_kernel(const __grid_constant__ TrainParams p) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   __shared__ Real s_red[2][2][kThreadsTarget / 32];   // [row parity][alpha, beta][warp]
   Real* s_buf = reinterpret_cast<Real*>(s_raw);
@@ -290,8 +292,14 @@ __global__ void __launch_bounds__(kThreadsTarget) train_backward_kernel(const __
   const int tid = threadIdx.x;
   const int g = tid / p.Zc, zx = tid - g * p.Zc;
   const bool active = g < p.G;
+  // LQ and dLQ of each code block in shared memory.  With kAlias they share
+  // one array (LQ while iteration t is recomputed, dLQ while it is
+  // back-propagated; between iterations dLQ waits in the block's own row of
+  // g_llr, which receives the final gradient at the end): half the shared
+  // memory per block, for configurations where that puts more blocks on an SM.
+  constexpr bool alias = kAlias;
   Real* lq = s_buf + (active ? g : 0) * p.n;
-  Real* glq = s_buf + (size_t)p.G * p.n + (active ? g : 0) * p.n;
+  Real* glq = alias ? lq : s_buf + (size_t)p.G * p.n + (active ? g : 0) * p.n;
   const size_t cw_words = (size_t)p.R * p.msg_words;
   const size_t edge_elems = (size_t)p.nnz * p.Zc;
   Real* tape = static_cast<Real*>(p.tape) + (size_t)blockIdx.x * p.scratch_per_cta + (size_t)(active ? g : 0) * edge_elems;
@@ -299,18 +307,20 @@ __global__ void __launch_bounds__(kThreadsTarget) train_backward_kernel(const __
   for (int item = blockIdx.x; item * p.G < p.batch; item += gridDim.x) {
     const int cw = item * p.G + g;
     const bool valid = active && cw < p.batch;
+    Real* stash = g_llr + (size_t)(valid ? cw : 0) * p.n;
+    Real* ginit = alias ? stash : glq;
     if (valid) {
-      for (int i = zx; i < p.n; i += p.Zc) glq[i] = g_final ? g_final[(size_t)cw * p.n + i] : (Real)0;
+      for (int i = zx; i < p.n; i += p.Zc) ginit[i] = g_final ? g_final[(size_t)cw * p.n + i] : (Real)0;
       for (size_t e = zx; e < edge_elems; e += p.Zc) carry[e] = 0;
     }
     __syncthreads();
     for (int t = p.T - 1; t >= 0; --t) {
-      if (valid) {
+      // every thread reads and writes only its own indices i = zx + k Zc here
+      if (valid)
         for (int i = zx; i < p.n; i += p.Zc) {
           lq[i] = ck_lq[((size_t)t * p.batch + cw) * p.n + i];
-          if (g_iter) glq[i] += g_iter[((size_t)t * p.batch + cw) * p.n + i];
+          if (!alias && g_iter) glq[i] += g_iter[((size_t)t * p.batch + cw) * p.n + i];
         }
-      }
       uint32_t* old_msg = (t > 0 && valid) ? p.ck_lr + ((size_t)t * p.batch + cw) * cw_words : nullptr;
       __syncthreads();
       // Recompute iteration t, keeping every rel on the tape.
@@ -321,6 +331,15 @@ __global__ void __launch_bounds__(kThreadsTarget) train_backward_kernel(const __
           NRLDPC_TRAIN_DISPATCH(train_row_fwd, Real, deg, p, lq, (uint32_t)zx, e0, row, alpha, beta, old_msg,
                                 nullptr, tape)
         }
+        __syncthreads();
+      }
+      if constexpr (alias) {
+        if (valid)
+          for (int i = zx; i < p.n; i += p.Zc) {
+            Real gq = stash[i];
+            if (g_iter) gq += g_iter[((size_t)t * p.batch + cw) * p.n + i];
+            glq[i] = gq;
+          }
         __syncthreads();
       }
       // Back-propagate through the rows of iteration t.
@@ -354,6 +373,8 @@ __global__ void __launch_bounds__(kThreadsTarget) train_backward_kernel(const __
           if (sb != (Real)0) atomicAdd(g_beta + t * p.R + row, sb);
         }
       }
+      if (alias && t > 0 && valid)
+        for (int i = zx; i < p.n; i += p.Zc) stash[i] = glq[i];   // own indices: no barrier needed
     }
     if (valid)
       for (int i = zx; i < p.n; i += p.Zc) {
@@ -395,20 +416,34 @@ int launch_train_forward(const TrainParams& p, bool f64, int grid, int block, in
 
 int launch_train_backward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream) {
   const bool bg2 = p.R == 42;
-  if (f64)
-    return bg2 ? launch_one(train_backward_kernel<double, 10>, p, grid, block, smem, stream)
-               : launch_one(train_backward_kernel<double, 19>, p, grid, block, smem, stream);
-  return bg2 ? launch_one(train_backward_kernel<float, 10>, p, grid, block, smem, stream)
-             : launch_one(train_backward_kernel<float, 19>, p, grid, block, smem, stream);
+  if (f64) {
+    if (p.alias)
+      return bg2 ? launch_one(train_backward_kernel<double, 10, true>, p, grid, block, smem, stream)
+                 : launch_one(train_backward_kernel<double, 19, true>, p, grid, block, smem, stream);
+    return bg2 ? launch_one(train_backward_kernel<double, 10, false>, p, grid, block, smem, stream)
+               : launch_one(train_backward_kernel<double, 19, false>, p, grid, block, smem, stream);
+  }
+  if (p.alias)
+    return bg2 ? launch_one(train_backward_kernel<float, 10, true>, p, grid, block, smem, stream)
+               : launch_one(train_backward_kernel<float, 19, true>, p, grid, block, smem, stream);
+  return bg2 ? launch_one(train_backward_kernel<float, 10, false>, p, grid, block, smem, stream)
+             : launch_one(train_backward_kernel<float, 19, false>, p, grid, block, smem, stream);
 }
 
-int occupancy_train(bool backward, bool f64, bool bg2, int block, int smem) {
+int occupancy_train(bool backward, bool f64, bool bg2, int block, int smem, bool alias) {
   if (backward) {
-    if (f64)
-      return bg2 ? occupancy_one(train_backward_kernel<double, 10>, block, smem)
-                 : occupancy_one(train_backward_kernel<double, 19>, block, smem);
-    return bg2 ? occupancy_one(train_backward_kernel<float, 10>, block, smem)
-               : occupancy_one(train_backward_kernel<float, 19>, block, smem);
+    if (f64) {
+      if (alias)
+        return bg2 ? occupancy_one(train_backward_kernel<double, 10, true>, block, smem)
+                   : occupancy_one(train_backward_kernel<double, 19, true>, block, smem);
+      return bg2 ? occupancy_one(train_backward_kernel<double, 10, false>, block, smem)
+                 : occupancy_one(train_backward_kernel<double, 19, false>, block, smem);
+    }
+    if (alias)
+      return bg2 ? occupancy_one(train_backward_kernel<float, 10, true>, block, smem)
+                 : occupancy_one(train_backward_kernel<float, 19, true>, block, smem);
+    return bg2 ? occupancy_one(train_backward_kernel<float, 10, false>, block, smem)
+               : occupancy_one(train_backward_kernel<float, 19, false>, block, smem);
   }
   if (f64)
     return bg2 ? occupancy_one(train_forward_kernel<double, 10>, block, smem)

@@ -415,7 +415,9 @@ int32_t nrldpc_train_forward(const float *d_llr, int32_t batch, const ldpc_in_co
  * of the final LLRs (d_g_final, nullable) and of every iteration's LLRs
  * (d_g_iter, nullable), writes d_g_llr [batch][N+2Zc] and ADDS into d_g_alpha /
  * d_g_beta [iterations][rows].  detach != 0 stops gradients through the check
- * update inputs (the model's detach_check_update_inputs). */
+ * update inputs (the model's detach_check_update_inputs).  d_g_llr also holds
+ * each block's running gradient between iterations, so it must not overlap
+ * d_llr, d_g_iter or the checkpoints (it may be d_g_final itself). */
 int32_t nrldpc_train_backward(const float *d_llr, int32_t batch, const ldpc_in_config_t *cfg,
                               int32_t iterations, const float *d_alpha, const float *d_beta,
                               float clip, int32_t detach, const float *d_ck_lq,
@@ -424,9 +426,9 @@ int32_t nrldpc_train_backward(const float *d_llr, int32_t batch, const ldpc_in_c
                               float *d_g_beta, void *stream);
 
 /* The same two kernels in float64, for gradient checks against finite
- * differences (float64 needs 2 (N+2Zc) doubles of shared memory per code block:
- * -2 where even one block does not fit, e.g. BG1 Zc > 208).  d_ck_lr is then
- * [iterations][batch][rows][6 Zc] uint32 words. */
+ * differences (float64 needs (N+2Zc) doubles of shared memory per code block:
+ * BG1 Zc = 384 still fits).  d_ck_lr is then [iterations][batch][rows][6 Zc]
+ * uint32 words. */
 int32_t nrldpc_train_forward_f64(const double *d_llr, int32_t batch, const ldpc_in_config_t *cfg,
                                  int32_t iterations, const double *d_alpha, const double *d_beta,
                                  double clip, double *d_final, double *d_iter, double *d_ck_lq,

@@ -164,13 +164,17 @@ def test_crc_targets_match_encoder(oracle, bgn, A, crc, E):
         assert np.array_equal(t[i], oracle.encode_codeword(pays[i], cfg)[: p.B])
 
 
-def test_training_checkpoint_sizes_and_float64_limit():
-    """BG1 Zc384 does not fit one float64 code block in shared memory: the entry
-    point refuses with the configuration error instead of launching."""
+def test_training_checkpoint_sizes_and_float64_fit():
+    """One code block of every configuration fits in shared memory, float64
+    included (BG1 Zc384: 26112 doubles, 209 KB, since the backward keeps LQ and
+    dLQ in one array); a configuration the parameter derivation rejects raises
+    instead of launching."""
     from deeplearning_5g_ldpc_decoder_b200 import capi
     from deeplearning_5g_ldpc_decoder_b200.train import checkpoint_sizes
 
+    lq, msg = checkpoint_sizes(capi.make_in_config(1, 8424, 1, 25344, 0, 2, 0), 2, 1, True)
+    assert lq == 2 * 1 * 68 * 384 and msg == 2 * 1 * 46 * 6 * 384
     with pytest.raises(ValueError):
-        checkpoint_sizes(capi.make_in_config(1, 8424, 1, 25344, 0, 2, 0), 2, 1, True)
+        checkpoint_sizes(capi.make_in_config(3, 8424, 1, 25344, 0, 2, 0), 2, 1, False)
     lq, msg = checkpoint_sizes(capi.make_in_config(1, 8424, 1, 25344, 0, 2, 0), 2, 3, False)
     assert lq == 2 * 3 * 68 * 384 and msg == 2 * 3 * 46 * 4 * 384
