@@ -336,10 +336,11 @@ int32_t decode_batch_locked(const int16_t* d_llr, int64_t llr_stride, int32_t nu
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (scratch_for(st, s, plan.scratch_bytes, &scratch) != 0) return NRLDPC_ERR_CUDA;
   DecodeParams& p = plan.p;
-  if (dc->algo >= 1 && dc->algo <= 3 && p.num_items > plan.grid) {
-    // More than one wave: half lanes refill from the stream's code-block queue
-    // (zeroed once, rewound by each launch's last CTA).  Within one wave there
-    // is nothing to refill from, and the fixed work items are a little faster.
+  if (p.num_items > plan.grid) {
+    // More than one wave: work comes from the stream's queue (zeroed once,
+    // rewound by each launch's last CTA): fixed point refills half lanes from
+    // it, the float kernels take work items from it.  Within one wave there is
+    // nothing to balance, and the fixed work items are a little faster.
     Buffer& q = st->queue[s];
     if (!q.ptr && (ensure(&q, 256) != 0 || cudaMemsetAsync(q.ptr, 0, 256, s) != cudaSuccess))
       return NRLDPC_ERR_CUDA;

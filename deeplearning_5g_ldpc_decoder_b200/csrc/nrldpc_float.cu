@@ -234,7 +234,16 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
   const int NT = p.nact;
   const int Bp = (p.B + 31) & ~31;
 
-  for (int item = blockIdx.x; item < p.num_items; item += gridDim.x) {
+  // Work items: fixed (item += grid) or, with a queue cursor, taken from the
+  // device queue so CTAs that run faster take more (see the fixed-point kernel).
+  __shared__ int s_item;
+  for (int item = blockIdx.x;;) {
+    if (p.cursor) {
+      if (tid == 0) s_item = atomicAdd(p.cursor, 1);
+      __syncthreads();
+      item = s_item;
+    }
+    if (item >= p.num_items) break;
     const int cw = item * p.G + g;
     const bool valid = active && cw < p.num_cw;
     if (active) {
@@ -288,7 +297,16 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
       }
     }
     if (active && !done) emit_float_block(p, lq, zx, cw, 1, it);
-    __syncthreads();
+    __syncthreads();   // LQ, s_crc and s_item are reused by the next item
+    if (!p.cursor) item += gridDim.x;
+  }
+  if (p.cursor && tid == 0) {
+    // every take of this CTA is done: the last CTA to finish rewinds the queue
+    __threadfence();
+    if (atomicAdd(p.cursor + 1, 1) == (int)gridDim.x - 1) {
+      atomicExch(p.cursor, 0);
+      atomicExch(p.cursor + 1, 0);
+    }
   }
 }
 

@@ -86,8 +86,8 @@ struct DecodeParams {
   int64_t harq_stride;
   uint32_t* scratch;
   int64_t scratch_words;   // per CTA
-  int32_t* cursor;         // fixed point: [queue head, finished CTAs], zero at launch, rewound by the
-                           // kernel's last CTA (null: fixed work items)
+  int32_t* cursor;         // work queue [head, finished CTAs]: zero at launch, rewound by the kernel's
+                           // last CTA (null: fixed work items)
   // Per edge: (base column * Zc) in the low 16 bits, (V_ij mod Zc) in the high.
   uint32_t edge[kMaxNnz];
   // The same two fields as byte offsets of 32-bit shared-memory words
