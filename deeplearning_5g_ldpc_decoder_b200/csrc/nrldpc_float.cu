@@ -115,6 +115,8 @@ __device__ __forceinline__ void fms_dispatch(int deg, const DecodeParams& p, flo
 }
 
 // --------------------------------------------------------------------- BP
+__device__ __forceinline__ void prefetch_l2(const void* a) { asm volatile("prefetch.global.L2 [%0];" ::"l"(a)); }
+
 __device__ __forceinline__ float bp_message(float prod) {
   // bp_message_from_product (:54-62)
   if (prod >= 1.0f) return 2.0f * kBpAtanhClip;
@@ -268,6 +270,15 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
           const int e0 = p.row_off[row];
           const int deg = p.row_off[row + 1] - e0;
           uint32_t* lrp = scratch + p.lr_off[row] + tid;
+          if constexpr (kBP) {
+            // The per-edge messages of the blocks in flight exceed L2, so their
+            // loads wait on DRAM: start moving the next row's (row 0 of the next
+            // iteration after the last row) toward L2 while this row computes.
+            const int rn = row + 1 < p.R ? row + 1 : 0;
+            const int dn = p.row_off[rn + 1] - p.row_off[rn];
+            const uint32_t* nx = scratch + p.lr_off[rn] + tid;
+            for (int j = 0; j < dn; ++j) prefetch_l2(nx + j * NT);
+          }
           if (kBP) {
             bp_dispatch(deg, p, lq, (uint32_t)zx, e0, it == 0, lrp, NT);
           } else {
