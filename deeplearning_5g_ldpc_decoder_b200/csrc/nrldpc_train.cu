@@ -49,6 +49,11 @@ __device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a
 template <typename Real>
 __device__ __forceinline__ Real r_inf() { return (Real)INFINITY; }
 
+// Start moving a line toward L2 (the checkpoints, tape and carry are read row
+// by row; issuing the next row's lines before the current row computes hides
+// part of their DRAM latency).
+__device__ __forceinline__ void prefetch_l2(const void* a) { asm volatile("prefetch.global.L2 [%0];" ::"l"(a)); }
+
 __device__ __forceinline__ uint32_t tr_addr(const TrainParams& p, int e, uint32_t zx) {
   const uint32_t ed = p.edge[e];
   uint32_t t = zx + (ed >> 16);
@@ -327,6 +332,11 @@ __global__ void __launch_bounds__(kThreadsTarget, (kMaxD > 10 || sizeof(Real) > 
       for (int row = 0; row < p.R; ++row) {
         if (valid) {
           const int e0 = p.row_off[row], deg = p.row_off[row + 1] - e0;
+          if (old_msg && row + 1 < p.R) {   // the next row's checkpointed messages
+            MsgBlock<Real> m(old_msg, row + 1, p.msg_words, p.Zc);
+            prefetch_l2(m.mag + zx);
+            prefetch_l2(m.bits + zx);
+          }
           const Real alpha = alpha_t[t * p.R + row], beta = beta_t[t * p.R + row];
           NRLDPC_TRAIN_DISPATCH(train_row_fwd, Real, deg, p, lq, (uint32_t)zx, e0, row, alpha, beta, old_msg,
                                 nullptr, tape)
@@ -347,6 +357,13 @@ __global__ void __launch_bounds__(kThreadsTarget, (kMaxD > 10 || sizeof(Real) > 
         Real ga = 0, gb = 0;
         if (valid) {
           const int e0 = p.row_off[row], deg = p.row_off[row + 1] - e0;
+          if (row > 0) {   // tape and carry of the row back-propagated next
+            const int ep = p.row_off[row - 1];
+            for (int j = 0; j < e0 - ep; ++j) {
+              prefetch_l2(tape + (size_t)(ep + j) * p.Zc + zx);
+              prefetch_l2(carry + (size_t)(ep + j) * p.Zc + zx);
+            }
+          }
           const Real alpha = alpha_t[t * p.R + row], beta = beta_t[t * p.R + row];
           NRLDPC_TRAIN_DISPATCH(train_row_bwd, Real, deg, p, glq, (uint32_t)zx, e0, alpha, beta, tape, carry, &ga,
                                 &gb)
