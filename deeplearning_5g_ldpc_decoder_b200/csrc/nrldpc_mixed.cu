@@ -52,10 +52,13 @@ __device__ __forceinline__ int32_t mixed_recover(const MixedGraph& g, const Mixe
   return s;
 }
 
-__device__ void mixed_emit(const MixedParams& p, const uint32_t* lq, int zx, int Zc, int cw, const MixedCw& c, int h,
-                           int status, int iters) {
+// The block descriptors are read from global memory where they are used
+// rather than kept in registers through the decode loop.
+__device__ void mixed_emit(const MixedParams& p, const uint32_t* lq, int zx, int Zc, int cw, int h, int status,
+                           int iters) {
   const int shift = 16 * h;
   if (iters > 0 && p.bits) {
+    const MixedCw& c = p.cws[cw];
     const int nbytes = (c.B + 7) >> 3;
     uint8_t* out = p.bits + c.bits_off;
     for (int byte = zx; byte < nbytes; byte += Zc) {
@@ -80,10 +83,11 @@ __device__ __forceinline__ int take_block(const MixedParams& p, int key) {
   return i < p.key_count[key] ? p.cb_list[p.key_base[key] + i] : -1;
 }
 
-// Rate recovery of one block into half h of the group's LQ words (the other
+// Rate recovery of block cw into half h of the group's LQ words (the other
 // half is kept), with its HARQ soft buffer.
-__device__ __forceinline__ void recover_half(const MixedParams& p, const MixedGraph& g, const MixedCw& c, int h,
-                                             uint32_t* lq, int zx) {
+__device__ __forceinline__ void recover_half(const MixedParams& p, const MixedGraph& g, int cw, int h, uint32_t* lq,
+                                             int zx) {
+  const MixedCw c = p.cws[cw];
   const int16_t* in = p.llr + c.llr_off;
   int16_t* hq = (c.harq_mode && p.harq) ? p.harq + c.harq_off : nullptr;
   const int shift = 16 * h;
@@ -129,17 +133,15 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
     __syncthreads();
     int cw[2] = {active ? s_cw[2 * g] : -1, active ? s_cw[2 * g + 1] : -1};
     if (__syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0))) continue;   // the graph's queue is empty
-    MixedCw c[2];
-    c[0] = cw[0] >= 0 ? p.cws[cw[0]] : MixedCw{};
-    c[1] = cw[1] >= 0 ? p.cws[cw[1]] : MixedCw{};
     int itv[2] = {0, 0};
     if (active) {
       if (zx == 0)
-        s_grp[g] = make_int4(cw[0] >= 0 ? c[0].B : 0, cw[1] >= 0 ? c[1].B : 0, c[0].crctype * kMaxB,
-                             c[1].crctype * kMaxB);
+        s_grp[g] = make_int4(cw[0] >= 0 ? p.cws[cw[0]].B : 0, cw[1] >= 0 ? p.cws[cw[1]].B : 0,
+                             cw[0] >= 0 ? p.cws[cw[0]].crctype * kMaxB : 0,
+                             cw[1] >= 0 ? p.cws[cw[1]].crctype * kMaxB : 0);
       for (int i = zx; i < lq_len; i += Zc) lq[i] = 0u;
       for (int h = 0; h < 2; ++h)
-        if (cw[h] >= 0) recover_half(p, s_g, c[h], h, lq, zx);
+        if (cw[h] >= 0) recover_half(p, s_g, cw[h], h, lq, zx);
     }
     if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
     uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
@@ -195,7 +197,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
           if (run) ++itv[h];
           const bool pass = run && s_crc[2 * g + h] == 0u;
           if (pass || itv[h] >= p.max_it) {
-            mixed_emit(p, lq, zx, Zc, cw[h], c[h], h, pass ? 0 : 1, itv[h]);
+            mixed_emit(p, lq, zx, Zc, cw[h], h, pass ? 0 : 1, itv[h]);
             refill[h] = true;
           }
         }
@@ -212,14 +214,14 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
           cw[h] = s_cw[2 * g + h];
           itv[h] = 0;
           if (cw[h] >= 0) {
-            c[h] = p.cws[cw[h]];
-            recover_half(p, s_g, c[h], h, lq, zx);
+            recover_half(p, s_g, cw[h], h, lq, zx);
             fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
           }
         }
         if (zx == 0 && (refill[0] || refill[1]))
-          s_grp[g] = make_int4(cw[0] >= 0 ? c[0].B : 0, cw[1] >= 0 ? c[1].B : 0, c[0].crctype * kMaxB,
-                               c[1].crctype * kMaxB);
+          s_grp[g] = make_int4(cw[0] >= 0 ? p.cws[cw[0]].B : 0, cw[1] >= 0 ? p.cws[cw[1]].B : 0,
+                               cw[0] >= 0 ? p.cws[cw[0]].crctype * kMaxB : 0,
+                               cw[1] >= 0 ? p.cws[cw[1]].crctype * kMaxB : 0);
       }
       if (__syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0))) break;
     }
