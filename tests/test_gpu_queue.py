@@ -69,3 +69,29 @@ def test_queue_and_fixed_items_decode_alike(oracle, cuda, algo):
         es, eb, ei, _ = oracle.decode(host[i], icfg, dec_cfg(row))
         assert (st[i], it[i]) == (es, ei), i
         assert np.array_equal(hb[i, : len(eb)], eb), i
+
+
+@pytest.mark.parametrize("algo", [1, 2, 0, 4])
+def test_queue_app_and_soft_buffers_alike(cuda, algo):
+    """With final beliefs requested and HARQ soft buffers combined into, a
+    queued launch (refilled half lanes, or queued work items for the float
+    kernels) leaves the same beliefs and the same soft buffers as launches of
+    fixed work items."""
+    cfg = CFG[:6] + (1,)                   # HARQ_on: combine into the soft buffers
+    row = [algo, 10, 22936, 0, 1280, 32767, -32767]
+    n = 8000 if algo in (1, 2) else 4000  # over two waves of either kernel
+    llr = _llrs(n, seed=70 + algo)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    harq0 = torch.randint(-200, 200, (n, 52 * 64), dtype=torch.int16, device="cuda", generator=gen)
+    ha, hb = harq0.clone(), harq0.clone()
+    full = ldpc_decode(llr, cfg, row, return_app=True, harq=ha)
+    chunk = 500
+    parts = [ldpc_decode(llr[i:i + chunk], cfg, row, return_app=True, harq=hb[i:i + chunk])
+             for i in range(0, n, chunk)]
+    torch.cuda.synchronize()
+    assert torch.equal(ha, hb)
+    assert not torch.equal(ha, harq0)
+    assert torch.equal(full.hardbits, torch.cat([p.hardbits for p in parts]))
+    assert torch.equal(full.iterations, torch.cat([p.iterations for p in parts]))
+    app = torch.cat([p.app for p in parts])
+    assert torch.equal(full.app, app)
