@@ -4,7 +4,8 @@
 //
 // Same arithmetic as the uniform kernel (nrldpc_fixed_row.cuh, bit-exact with
 // c_lib/fixedpoint_ldpc_decoder.c).  Differences:
-//  * work items come from a device work queue (atomic counter); an item is a
+//  * work items come from a device work queue (atomic counter, after each
+//    CTA's first item, which is its own index); an item is a
 //    CTA's claim on one (BG, Zc), whose tables (per-edge shared-memory offsets,
 //    row offsets, scratch layout) are staged into shared memory;
 //  * the CTA takes up to 2G blocks of that graph from the graph's block queue
@@ -112,8 +113,14 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
   const int tid = threadIdx.x;
   uint32_t* scratch = p.scratch + (int64_t)blockIdx.x * p.scratch_words;
   const int num_items = p.num_items_dev ? *p.num_items_dev : p.num_items;
+  // A CTA's first claim is its own index and later ones come from the queue:
+  // CTAs are placed on the SMs breadth first, so a batch with fewer claims
+  // than SMs gets one SM per claim instead of whichever CTAs reach the queue
+  // first (two of them may share an SM), which shortens small batches.
+  bool first = true;
   for (;;) {
-    if (tid == 0) s_item = atomicAdd(p.counter, 1);
+    if (tid == 0) s_item = first ? (int)blockIdx.x : (int)gridDim.x + atomicAdd(p.counter, 1);
+    first = false;
     __syncthreads();
     const int item = s_item;
     if (item >= num_items) break;
