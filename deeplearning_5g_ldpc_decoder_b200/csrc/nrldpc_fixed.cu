@@ -183,9 +183,13 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
     uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
     bool idle = __syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0));
     const bool run = p.max_it > 0;   // max_iterations == 0: rate recovery only, status 1
+    RowMsg nxt{};
     while (!idle) {
       for (int row = 0; run && row < p.R; ++row) {
         if (active) {
+          const RowMsg cur = nxt;
+          const int rn = row + 1 < p.R ? row + 1 : 0;
+          nxt = load_row_msg(scratch + p.lr_off[rn] + tid, p.lr_off[rn + 1] - p.lr_off[rn] > 4u * kThreadsTarget);
           const int e0 = p.row_off[row];
           const int deg = p.row_off[row + 1] - e0;
           uint32_t ab0, ab1;
@@ -197,7 +201,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
           }
           layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0,
                                            (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
-                                           (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, fresh,
+                                           (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, cur, fresh,
                                            scratch + p.lr_off[row] + tid);
         }
         __syncthreads();
@@ -280,9 +284,13 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
       __syncthreads();
 
       int it = 0;
+      RowMsg nxt{};
       for (; it < p.max_it; ++it) {
         for (int row = 0; row < p.R; ++row) {
           if (active) {
+            const RowMsg cur = nxt;
+            const int rn = row + 1 < p.R ? row + 1 : 0;
+            nxt = load_row_msg(scratch + p.lr_off[rn] + tid, p.lr_off[rn + 1] - p.lr_off[rn] > 4u * kThreadsTarget);
             const int e0 = p.row_off[row];
             const int deg = p.row_off[row + 1] - e0;
             const uint32_t ab = p.weights_T > 0 ? __ldg(p.weights + (min(it, p.weights_T - 1) * p.R + row))
@@ -290,7 +298,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
             const int32_t alpha = (int32_t)(int16_t)(ab & 0xFFFFu);
             const int32_t beta = ((int32_t)ab) >> 16;
             layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0, alpha, beta,
-                                             alpha, beta, it == 0 ? 0xFFFFFFFFu : 0u, scratch + p.lr_off[row] + tid);
+                                             alpha, beta, cur, it == 0 ? 0xFFFFFFFFu : 0u, scratch + p.lr_off[row] + tid);
           }
           __syncthreads();
         }

@@ -76,20 +76,37 @@ __device__ __forceinline__ uint32_t cond_neg16x2(uint32_t v, uint32_t m) { retur
 // Instruction budget: packed add/sub run on the FMA pipe, packed min/max,
 // PRMT and LOP3 on the ALU pipe (the bottleneck); the emulated saturating
 // packed ops are kept off the common path.
+// The compressed old message words of one lifted row (w0..w4 below), loaded
+// by the kernels one row ahead so that their L2 latency overlaps the row
+// before.
+struct RowMsg {
+  uint32_t n1, n2, xf, xi, y;
+};
+__device__ __forceinline__ RowMsg load_row_msg(const uint32_t* lrp, bool five) {
+  constexpr int S = kThreadsTarget;
+  RowMsg m;
+  m.n1 = lrp[0];
+  m.n2 = lrp[S];
+  m.xf = lrp[2 * S];
+  m.xi = lrp[3 * S];
+  m.y = five ? lrp[4 * S] : 0u;
+  return m;
+}
+
 template <int D, bool kDegenClip, bool kSmemEdges, typename P>
 __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__ sedges, char* __restrict__ lqs, uint32_t zx4,
                                            uint32_t zxm4, uint32_t gb4, int e0, int32_t alpha, int32_t beta,
-                                           int32_t alpha1, int32_t beta1, uint32_t fresh,
+                                           int32_t alpha1, int32_t beta1, const RowMsg& old, uint32_t fresh,
                                            uint32_t* __restrict__ lrp) {
   constexpr int J = D < 16 ? D : 16;
   constexpr int S = kThreadsTarget;    // plane stride (words)
   uint32_t n1 = 0u, n2 = 0u, xf = 0u, xi = 0u, y = 0u;
   if (fresh != 0xFFFFFFFFu) {
-    n1 = lrp[0];
-    n2 = lrp[S];
-    xf = lrp[2 * S];
-    xi = lrp[3 * S];
-    if (D > 16) y = lrp[4 * S];
+    n1 = old.n1;
+    n2 = old.n2;
+    xf = old.xf;
+    xi = old.xi;
+    if (D > 16) y = old.y;
     if (fresh) {
       const uint32_t keep = ~fresh;
       n1 &= keep;
@@ -210,10 +227,11 @@ __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__
 template <bool kDegenClip, bool kSmemEdges, typename P>
 __device__ __forceinline__ void layer_dispatch(int deg, const P& p, const uint2* sedges, char* lqs, uint32_t zx4, uint32_t zxm4,
                                                uint32_t gb4, int e0, int32_t alpha, int32_t beta,
-                                               int32_t alpha1, int32_t beta1, uint32_t fresh, uint32_t* lrp) {
+                                               int32_t alpha1, int32_t beta1, const RowMsg& old, uint32_t fresh,
+                                               uint32_t* lrp) {
   switch (deg) {
 #define NRLDPC_ROW(D) \
-  case D: row_update<D, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, alpha1, beta1, fresh, lrp); break;
+  case D: row_update<D, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, alpha1, beta1, old, fresh, lrp); break;
     NRLDPC_ROW(3)
     NRLDPC_ROW(4)
     NRLDPC_ROW(5)
@@ -223,7 +241,7 @@ __device__ __forceinline__ void layer_dispatch(int deg, const P& p, const uint2*
     NRLDPC_ROW(9)
     NRLDPC_ROW(10)
 #undef NRLDPC_ROW
-    default: row_update<19, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, alpha1, beta1, fresh, lrp); break;
+    default: row_update<19, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, alpha1, beta1, old, fresh, lrp); break;
   }
 }
 

@@ -159,10 +159,14 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
     const uint32_t zxm4 = zx4 - 4u * (uint32_t)Zc;
     const uint32_t gb4 = 4u * (uint32_t)((active ? g : 0) * lq_len);
     const int Bp = (s_g.K + 31) & ~31;   // every block's B <= K
+    RowMsg nxt{};
     for (;;) {
       const bool run = p.max_it > 0;   // max_iterations == 0: rate recovery only, status 1
       for (int row = 0; run && row < s_g.R; ++row) {
         if (active) {
+          const RowMsg cur = nxt;
+          const int rn = row + 1 < s_g.R ? row + 1 : 0;
+          nxt = load_row_msg(scratch + s_g.lr_off[rn] + tid, s_g.lr_off[rn + 1] - s_g.lr_off[rn] > 4u * kThreadsTarget);
           const int e0 = s_g.row_off[row];
           const int deg = s_g.row_off[row + 1] - e0;
           uint32_t ab0, ab1;
@@ -174,7 +178,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
           }
           layer_dispatch<kDegenClip, true>(deg, p, s_g.edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0,
                                            (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
-                                           (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, fresh,
+                                           (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, cur, fresh,
                                            scratch + s_g.lr_off[row] + tid);
         }
         __syncthreads();
