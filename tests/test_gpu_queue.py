@@ -95,3 +95,24 @@ def test_queue_app_and_soft_buffers_alike(cuda, algo):
     assert torch.equal(full.iterations, torch.cat([p.iterations for p in parts]))
     app = torch.cat([p.app for p in parts])
     assert torch.equal(full.app, app)
+
+
+@pytest.mark.parametrize("algo", [1, 4])
+def test_queue_zero_iterations_alike(cuda, algo):
+    """max_iterations == 0 (rate recovery only, status 1, bits untouched): a
+    queued launch and fixed-item launches leave the same beliefs, soft buffers
+    and outputs."""
+    cfg = CFG[:6] + (1,)
+    row = [algo, 0, 22936, 0, 1280, 32767, -32767]
+    n = 8000
+    llr = _llrs(n, seed=90 + algo)
+    gen = torch.Generator(device="cuda").manual_seed(9)
+    harq0 = torch.randint(-200, 200, (n, 52 * 64), dtype=torch.int16, device="cuda", generator=gen)
+    ha, hb = harq0.clone(), harq0.clone()
+    full = ldpc_decode(llr, cfg, row, return_app=True, harq=ha)
+    parts = [ldpc_decode(llr[i:i + 500], cfg, row, return_app=True, harq=hb[i:i + 500]) for i in range(0, n, 500)]
+    torch.cuda.synchronize()
+    assert torch.equal(ha, hb) and not torch.equal(ha, harq0)
+    assert bool((full.status == 1).all()) and bool((full.iterations == 0).all())
+    assert not bool(full.hardbits.any())
+    assert torch.equal(full.app, torch.cat([p.app for p in parts]))
