@@ -132,7 +132,7 @@ struct DeviceState {
   struct HostStage {
     Buffer llr, bits, stat, iters;
     cudaStream_t copy = nullptr;                   // copy-engine stream of the pipeline
-    cudaStream_t comp[2] = {nullptr, nullptr};     // decode streams: chunks alternate between them
+    cudaStream_t comp[4] = {nullptr, nullptr, nullptr, nullptr};   // decode streams: chunks rotate over them
     cudaEvent_t start = nullptr;
     std::vector<cudaEvent_t> h2d, dec;             // per chunk
   };
@@ -710,27 +710,34 @@ int32_t nrldpc_decode_batch_host(const int16_t* h_llr, int64_t llr_stride, int32
     if (cudaStreamCreateWithFlags(&hs.copy, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&hs.comp[0], cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&hs.comp[1], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&hs.comp[2], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&hs.comp[3], cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&hs.start, cudaEventDisableTiming) != cudaSuccess)
       return NRLDPC_ERR_CUDA;
   }
-  // Chunks of whole waves of the decode kernel: chunk k+1's host-to-device copy
-  // overlaps chunk k's decode, and the waves of the chunks add up to the waves of
-  // one launch over the whole batch, so nothing is lost to partial waves.
-  // Consecutive chunks decode on two streams, so the CTAs of chunk k+1 start on
-  // the SMs that chunk k's first finishers leave free (no tail per chunk).
+  // Chunks: chunk k+1's host-to-device copy overlaps the decode of the chunks
+  // before it.  The first three are a quarter, a quarter and half a kernel
+  // wave, the rest whole waves (at most 32 chunks): the first copy, the only
+  // one nothing hides, is small, and decoding starts while the next chunks
+  // arrive.  Chunks rotate over four decode streams, so the small first chunks
+  // run side by side and every chunk's CTAs start on the SMs that earlier
+  // chunks' finishers leave free (no tail per chunk).
   Plan probe;
   if (make_plan(cp, *decoder_cfg, num_cw, st, &probe) != 0) return NRLDPC_ERR_CUDA;
   const bool fixed = decoder_cfg->algo >= 1 && decoder_cfg->algo <= 3;
   const int64_t wave_cw = (int64_t)(fixed ? 2 : 1) * probe.p.G * probe.grid;
-  // One wave per chunk (at most 32 chunks): the copy of the first chunk is the
-  // only one not hidden behind a decode.
-  int64_t chunk = num_cw;
+  std::vector<int64_t> cuts{0};   // chunk k covers blocks [cuts[k], cuts[k+1])
   constexpr int kMaxChunks = 32;
-  if (wave_cw > 0 && num_cw >= 3 * wave_cw) {
-    const int64_t want = (num_cw + kMaxChunks - 1) / kMaxChunks;
-    chunk = std::max<int64_t>(wave_cw, (want + wave_cw - 1) / wave_cw * wave_cw);
+  if (wave_cw >= 8 && num_cw >= 3 * wave_cw) {
+    const int64_t q = (wave_cw / 4 + 1) & ~(int64_t)1;   // even: whole lane pairs
+    const int64_t want = (num_cw + kMaxChunks - 4) / (kMaxChunks - 3);
+    const int64_t body = std::max<int64_t>(wave_cw, (want + wave_cw - 1) / wave_cw * wave_cw);
+    for (const int64_t c : {q, q, 2 * q}) cuts.push_back(cuts.back() + c);
+    while (cuts.back() < num_cw) cuts.push_back(std::min<int64_t>(num_cw, cuts.back() + body));
+  } else {
+    cuts.push_back(num_cw);
   }
-  const int nchunks = (int)((num_cw + chunk - 1) / chunk);
+  const int nchunks = (int)cuts.size() - 1;
   while ((int)hs.h2d.size() < nchunks) {
     cudaEvent_t a, b;
     if (cudaEventCreateWithFlags(&a, cudaEventDisableTiming) != cudaSuccess ||
@@ -742,14 +749,16 @@ int32_t nrldpc_decode_batch_host(const int16_t* h_llr, int64_t llr_stride, int32
   // work already queued on the caller's stream comes first
   if (cudaEventRecord(hs.start, s) != cudaSuccess || cudaStreamWaitEvent(hs.copy, hs.start, 0) != cudaSuccess ||
       cudaStreamWaitEvent(hs.comp[0], hs.start, 0) != cudaSuccess ||
-      cudaStreamWaitEvent(hs.comp[1], hs.start, 0) != cudaSuccess)
+      cudaStreamWaitEvent(hs.comp[1], hs.start, 0) != cudaSuccess ||
+      cudaStreamWaitEvent(hs.comp[2], hs.start, 0) != cudaSuccess ||
+      cudaStreamWaitEvent(hs.comp[3], hs.start, 0) != cudaSuccess)
     return NRLDPC_ERR_CUDA;
   int16_t* d_llr = static_cast<int16_t*>(hs.llr.ptr);
   uint8_t* d_bits = static_cast<uint8_t*>(hs.bits.ptr);
   int32_t* d_stat = static_cast<int32_t*>(hs.stat.ptr);
   int32_t* d_iters = static_cast<int32_t*>(hs.iters.ptr);
   for (int k = 0; k < nchunks; ++k) {
-    const int64_t c0 = k * chunk, n = std::min<int64_t>(chunk, num_cw - c0);
+    const int64_t c0 = cuts[k], n = cuts[k + 1] - cuts[k];
     const size_t off = (size_t)c0 * (size_t)llr_stride;
     if (cudaMemcpyAsync(d_llr + off, h_llr + off, sizeof(int16_t) * (size_t)n * (size_t)llr_stride,
                         cudaMemcpyHostToDevice, hs.copy) != cudaSuccess ||
@@ -757,8 +766,8 @@ int32_t nrldpc_decode_batch_host(const int16_t* h_llr, int64_t llr_stride, int32
       return NRLDPC_ERR_CUDA;
   }
   for (int k = 0; k < nchunks; ++k) {
-    const int64_t c0 = k * chunk, n = std::min<int64_t>(chunk, num_cw - c0);
-    cudaStream_t comp = hs.comp[k & 1];
+    const int64_t c0 = cuts[k], n = cuts[k + 1] - cuts[k];
+    cudaStream_t comp = hs.comp[k & 3];
     if (cudaStreamWaitEvent(comp, hs.h2d[k], 0) != cudaSuccess) return NRLDPC_ERR_CUDA;
     const int32_t rc = decode_batch_locked(d_llr + (size_t)c0 * (size_t)llr_stride, llr_stride, (int32_t)n, inconfig,
                                            decoder_cfg, d_bits + (size_t)c0 * (size_t)bits_stride, bits_stride,

@@ -164,9 +164,10 @@ def test_algo2_beyond_table_reuses_last_row(oracle, cuda):
 
 @pytest.mark.parametrize("algo", [1, 4])
 def test_host_buffer_pipeline_matches_device_path(oracle, cuda, algo):
-    """nrldpc_decode_batch_host copies and decodes in overlapped chunks of whole
-    kernel waves; results equal the device-pointer path for batches below,
-    at and well above the chunking threshold, and a sample equals the oracle."""
+    """nrldpc_decode_batch_host copies and decodes in overlapped chunks (a
+    quarter, a quarter and half a kernel wave, then whole waves, on four decode
+    streams); results equal the device-pointer path for batches below, at and
+    well above the chunking threshold, and a sample equals the oracle."""
     from deeplearning_5g_ldpc_decoder_b200 import ldpc_decode_host
 
     cfg = (2, 488, 1, 1920, 0, 2, 0)
