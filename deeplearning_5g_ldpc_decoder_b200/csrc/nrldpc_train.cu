@@ -179,7 +179,53 @@ __device__ __forceinline__ void train_row_bwd(const TrainParams& p, Real* __rest
   const Real k2 = o2 >= (Real)0 ? alpha : (Real)0;
   const Real s1 = r_mul(alpha, r1), s2 = r_mul(alpha, r2);
   Real g_a_idx = 0, g_a_idx2 = 0;
-  Real g_new[D], g_mag_sum_r = 0, g_u_sum = 0;
+  Real g_mag_sum_r = 0, g_u_sum = 0;
+  if constexpr (D > 10) {
+    // Degree-19 rows keep only rel in registers: the edge addresses are
+    // recomputed and the incoming gradient g_v is read again from shared
+    // memory in the last pass (no other edge of the row writes that word),
+    // so the BG1 kernel fits two CTAs per SM.  Same arithmetic as below.
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      const uint32_t a = tr_addr(p, e0 + j, zx);
+      const bool flip = (rel[j] < (Real)0) != neg;
+      const Real mag = (j == idx) ? s2 : s1;
+      const Real v = r_add(rel[j], flip ? -mag : mag);
+      const Real gv = (v >= -clip && v <= clip) ? glq[a] : (Real)0;
+      const Real g_lrt = carry[(size_t)(e0 + j) * Zc + zx] + gv;
+      const Real g_mag = flip ? -g_lrt : g_lrt;
+      g_mag_sum_r += g_mag * ((j == idx) ? r2 : r1);
+      const Real g_u = g_mag * ((j == idx) ? k2 : k1);
+      g_u_sum += g_u;
+      if (j == idx) {
+        g_a_idx2 += g_u;
+      } else {
+        g_a_idx += g_u;
+      }
+    }
+    *ga += g_mag_sum_r;
+    *gb -= g_u_sum;
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      const uint32_t a = tr_addr(p, e0 + j, zx);
+      Real g_rel = 0;
+      if (!p.detach) {
+        const bool flip = (rel[j] < (Real)0) != neg;
+        const Real mag = (j == idx) ? s2 : s1;
+        const Real v = r_add(rel[j], flip ? -mag : mag);
+        const Real gv = (v >= -clip && v <= clip) ? glq[a] : (Real)0;
+        Real g_a = 0;
+        if (j == idx) g_a += g_a_idx;
+        if (j == idx2) g_a += g_a_idx2;
+        const Real sg = rel[j] > (Real)0 ? (Real)1 : (rel[j] < (Real)0 ? (Real)-1 : (Real)0);
+        g_rel = gv + g_a * sg;
+      }
+      glq[a] = g_rel;
+      carry[(size_t)(e0 + j) * Zc + zx] = -g_rel;
+    }
+    return;
+  }
+  Real g_new[D];
 #pragma unroll
   for (int j = 0; j < D; ++j) {
     const bool flip = (rel[j] < (Real)0) != neg;
@@ -277,9 +323,9 @@ __global__ void __launch_bounds__(kThreadsTarget) train_forward_kernel(const __g
   }
 }
 
-// Float BG2 (kMaxD 10): at most 85 registers, so two 384-thread CTAs fit an SM.
+// Float: at most 85 registers, so two 384-thread CTAs fit an SM.
 template <typename Real, int kMaxD, bool kAlias>
-__global__ void __launch_bounds__(kThreadsTarget, (kMaxD > 10 || sizeof(Real) > 4) ? 1 : 2)
+__global__ void __launch_bounds__(kThreadsTarget, sizeof(Real) > 4 ? 1 : 2)
     train_backward_kernel(const __grid_constant__ TrainParams p) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   __shared__ Real s_red[2][2][kThreadsTarget / 32];   // [row parity][alpha, beta][warp]
