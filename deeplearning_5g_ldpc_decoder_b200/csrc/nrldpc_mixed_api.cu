@@ -1,6 +1,6 @@
-// nrldpc_mixed_api.cu — host side of mixed-size batches: the plan (pairing of
-// blocks of one (BG, Zc), work items, device tables), its CUDA graph, and a
-// small autotuner over the launch shape and the work-item order.
+// nrldpc_mixed_api.cu — host side of mixed-size batches: the plan (one block
+// queue per (BG, Zc), work items claiming them, device tables), its CUDA
+// graph, and a small autotuner over the launch shape and the work-item order.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -21,7 +21,7 @@ struct MixedPlanImpl {
   int num_sms = 0;
   bool degen = false;
   std::vector<MixedGraph> graphs;
-  std::vector<std::vector<int>> members;   // block indices per graph, in pairing order
+  std::vector<std::vector<int>> members;   // block indices per graph, in queue order
   std::vector<MixedCw> cws;
   MixedGraph* d_graphs = nullptr;
   MixedCw* d_cws = nullptr;
