@@ -223,42 +223,42 @@ __device__ __forceinline__ void train_row_bwd(const TrainParams& p, Real* __rest
       glq[a] = g_rel;
       carry[(size_t)(e0 + j) * Zc + zx] = -g_rel;
     }
-    return;
-  }
-  Real g_new[D];
+  } else {
+    Real g_new[D];
 #pragma unroll
-  for (int j = 0; j < D; ++j) {
-    const bool flip = (rel[j] < (Real)0) != neg;
-    const Real mag = (j == idx) ? s2 : s1;
-    const Real v = r_add(rel[j], flip ? -mag : mag);
-    const Real gv = (v >= -clip && v <= clip) ? glq[addr[j]] : (Real)0;
-    g_new[j] = gv;
-    Real* cr = carry + (size_t)(e0 + j) * Zc + zx;
-    const Real g_lrt = *cr + gv;
-    const Real g_mag = flip ? -g_lrt : g_lrt;
-    g_mag_sum_r += g_mag * ((j == idx) ? r2 : r1);
-    const Real g_u = g_mag * ((j == idx) ? k2 : k1);
-    g_u_sum += g_u;
-    if (j == idx) {
-      g_a_idx2 += g_u;
-    } else {
-      g_a_idx += g_u;
+    for (int j = 0; j < D; ++j) {
+      const bool flip = (rel[j] < (Real)0) != neg;
+      const Real mag = (j == idx) ? s2 : s1;
+      const Real v = r_add(rel[j], flip ? -mag : mag);
+      const Real gv = (v >= -clip && v <= clip) ? glq[addr[j]] : (Real)0;
+      g_new[j] = gv;
+      Real* cr = carry + (size_t)(e0 + j) * Zc + zx;
+      const Real g_lrt = *cr + gv;
+      const Real g_mag = flip ? -g_lrt : g_lrt;
+      g_mag_sum_r += g_mag * ((j == idx) ? r2 : r1);
+      const Real g_u = g_mag * ((j == idx) ? k2 : k1);
+      g_u_sum += g_u;
+      if (j == idx) {
+        g_a_idx2 += g_u;
+      } else {
+        g_a_idx += g_u;
+      }
     }
-  }
-  *ga += g_mag_sum_r;
-  *gb -= g_u_sum;
+    *ga += g_mag_sum_r;
+    *gb -= g_u_sum;
 #pragma unroll
-  for (int j = 0; j < D; ++j) {
-    Real g_rel = 0;
-    if (!p.detach) {
-      Real g_a = 0;
-      if (j == idx) g_a += g_a_idx;
-      if (j == idx2) g_a += g_a_idx2;
-      const Real sg = rel[j] > (Real)0 ? (Real)1 : (rel[j] < (Real)0 ? (Real)-1 : (Real)0);
-      g_rel = g_new[j] + g_a * sg;
+    for (int j = 0; j < D; ++j) {
+      Real g_rel = 0;
+      if (!p.detach) {
+        Real g_a = 0;
+        if (j == idx) g_a += g_a_idx;
+        if (j == idx2) g_a += g_a_idx2;
+        const Real sg = rel[j] > (Real)0 ? (Real)1 : (rel[j] < (Real)0 ? (Real)-1 : (Real)0);
+        g_rel = g_new[j] + g_a * sg;
+      }
+      glq[addr[j]] = g_rel;
+      carry[(size_t)(e0 + j) * Zc + zx] = -g_rel;
     }
-    glq[addr[j]] = g_rel;
-    carry[(size_t)(e0 + j) * Zc + zx] = -g_rel;
   }
 }
 
