@@ -28,8 +28,11 @@
 //    max_iterations the block's outputs are written and the half lane
 //    restarts on the next block (zero messages through the `fresh` mask, its
 //    own iteration count), so each block costs its own iterations.  Without a
-//    cursor (the no-allocation entry point) each CTA loops over fixed work
-//    items of G pairs until every block of the item has finished.
+//    cursor (launches of one wave or less, and the no-allocation entry point)
+//    each CTA loops over fixed work items of G pairs until every block of the
+//    item has finished.
+//  * Each row's compressed message words are loaded while the row before it
+//    computes (load_row_msg), hiding their L2 latency.
 //  * CRC early termination runs every iteration inside the kernel: each hard
 //    bit i contributes x^(B-1-i+W) mod g(x) (a precomputed table), the
 //    contributions are XOR-reduced with warp reductions and shared atomics.
