@@ -176,9 +176,11 @@ int32_t nrldpc_decode_batch(const int16_t *d_llr, int64_t llr_stride,
                             void *stream);
 
 /* Same as nrldpc_decode_batch, from and to HOST memory: copies the LLRs in,
- * decodes, copies hard bits / status / iterations back and synchronises the
- * stream.  Pinned host buffers give full copy bandwidth.  h_status and
- * h_iterations are nullable. */
+ * decodes, copies hard bits / status / iterations back, and returns once they
+ * are in host memory (the work starts after what is already queued on
+ * `stream`; copies and decodes overlap in chunks on internal streams).
+ * Pinned host buffers give full copy bandwidth.  h_status and h_iterations
+ * are nullable. */
 int32_t nrldpc_decode_batch_host(const int16_t *h_llr, int64_t llr_stride,
                                  int32_t num_cw,
                                  const ldpc_in_config_t *inconfig,
