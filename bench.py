@@ -782,7 +782,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--algo", type=int, default=1, choices=[0, 1, 2, 3, 4],
                     help="decoder of the main step (profiling of the other kernels; the headline is algo 1)")
-    ap.add_argument("--pipeline-depth", type=int, default=6, help="serve: batches in flight (streams)")
+    ap.add_argument("--pipeline-depth", type=int, default=8, help="serve: batches in flight (streams)")
     ap.add_argument("--workload", default="bg1_zc384", choices=["bg1_zc384", "mixed", "train", "serve"],
                     help="mixed: 32768 blocks over all 51 lifting sizes, BG1 60 %%, rate U[0.2, 0.92], Qm 2-8; "
                          "train: learned min-sum forward+backward, batch 4096, 10 iterations")

@@ -619,7 +619,7 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
   TbEngine* e = static_cast<TbEngine*>(engine);
   if (!e || !cfg || n < 0 || (n > 0 && (!tbs || !arrival_s || !d_llr || !d_out || !h_status || !h_latency_s)))
     return NRLDPC_ERR_ARG;
-  const int depth = std::max(1, std::min(8, cfg->pipeline_depth));
+  const int depth = std::max(1, std::min(16, cfg->pipeline_depth));
   const int max_tbs = std::max(1, std::min(cfg->max_batch_tbs, e->max_tbs));
   const int max_cbs = std::max(1, std::min(cfg->max_batch_cbs, e->max_cbs));
   for (int i = 1; i < n; ++i)

@@ -371,7 +371,7 @@ typedef struct {
     int32_t max_batch_tbs;      /* transport blocks per decode batch at most */
     int32_t max_batch_cbs;      /* code blocks per decode batch at most */
     int64_t llr_budget_bytes;   /* HBM for the LLRs of admitted, unfinished blocks */
-    int32_t pipeline_depth;     /* batches in flight, 1..8 */
+    int32_t pipeline_depth;     /* batches in flight, 1..16 (one engine lane each: ~90 MB of scratch) */
     int32_t pad;
     double timeout_s;           /* the run fails with NRLDPC_ERR_CUDA after this long */
 } nrldpc_serve_cfg_t;
