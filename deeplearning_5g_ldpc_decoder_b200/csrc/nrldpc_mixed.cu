@@ -213,8 +213,10 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
           }
         }
       }
-      __syncthreads();   // s_crc read and emits done before the lanes are refilled
+      // s_crc read and emits done before the lanes are refilled
+      const bool any = __syncthreads_or(refill[0] || refill[1]);
       if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
+      if (!any) continue;   // nothing finished: the next iteration (the rows' barriers order s_crc)
       if (active && zx == 0)
         for (int h = 0; h < 2; ++h)
           if (refill[h]) s_cw[2 * g + h] = take_block(p, key);
