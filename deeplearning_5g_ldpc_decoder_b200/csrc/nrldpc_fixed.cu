@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
       cw[1] = s_base + 2 * g + 1 < p.num_cw ? s_base + 2 * g + 1 : -1;
       recover_halves(p, lq, zx, cw[0], cw[1], true, true);
     }
-    int itv[2] = {0, 0};
+    uint32_t itv = 0u;   // iterations of half 0 in bits 0-15, half 1 in bits 16-31
     if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
     uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
     bool idle = __syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0));
@@ -197,8 +197,8 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
           const int deg = p.row_off[row + 1] - e0;
           uint32_t ab0, ab1;
           if (p.weights_T > 0) {
-            ab0 = __ldg(p.weights + (min(itv[0], p.weights_T - 1) * p.R + row));
-            ab1 = __ldg(p.weights + (min(itv[1], p.weights_T - 1) * p.R + row));
+            ab0 = __ldg(p.weights + (min((int)(itv & 0xFFFFu), p.weights_T - 1) * p.R + row));
+            ab1 = __ldg(p.weights + (min((int)(itv >> 16), p.weights_T - 1) * p.R + row));
           } else {
             ab0 = ab1 = p.w_inline[row];
           }
@@ -216,10 +216,11 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
       if (active) {
         for (int h = 0; h < 2; ++h) {
           if (cw[h] < 0) continue;
-          if (run) ++itv[h];
+          if (run) itv += h ? 0x10000u : 1u;
+          const int ith = (int)(h ? itv >> 16 : itv & 0xFFFFu);
           const bool pass = run && s_crc[2 * g + h] == 0u;
-          if (pass || itv[h] >= p.max_it) {
-            emit_block(p, lq, zx, cw[h], h, pass ? 0 : 1, itv[h]);
+          if (pass || ith >= p.max_it) {
+            emit_block(p, lq, zx, cw[h], h, pass ? 0 : 1, ith);
             fin[h] = true;
           }
         }
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
         for (int h = 0; h < 2; ++h) {
           if (!fin[h]) continue;
           cw[h] = s_cw[2 * g + h];
-          itv[h] = 0;
+          itv &= h ? 0x0000FFFFu : 0xFFFF0000u;
           if (cw[h] >= 0) fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
         }
         recover_halves(p, lq, zx, cw[0], cw[1], fin[0], fin[1]);

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
     __syncthreads();
     int cw[2] = {active ? s_cw[2 * g] : -1, active ? s_cw[2 * g + 1] : -1};
     if (__syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0))) continue;   // the graph's queue is empty
-    int itv[2] = {0, 0};
+    uint32_t itv = 0u;   // iterations of half 0 in bits 0-15, half 1 in bits 16-31
     if (active) {
       if (zx == 0)
         s_grp[g] = make_int4(cw[0] >= 0 ? p.cws[cw[0]].B : 0, cw[1] >= 0 ? p.cws[cw[1]].B : 0,
@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
           const int deg = s_g.row_off[row + 1] - e0;
           uint32_t ab0, ab1;
           if (p.weights_T[bi] > 0) {
-            ab0 = __ldg(p.weights[bi] + (min(itv[0], p.weights_T[bi] - 1) * s_g.R + row));
-            ab1 = __ldg(p.weights[bi] + (min(itv[1], p.weights_T[bi] - 1) * s_g.R + row));
+            ab0 = __ldg(p.weights[bi] + (min((int)(itv & 0xFFFFu), p.weights_T[bi] - 1) * s_g.R + row));
+            ab1 = __ldg(p.weights[bi] + (min((int)(itv >> 16), p.weights_T[bi] - 1) * s_g.R + row));
           } else {
             ab0 = ab1 = p.w_inline[bi][row];
           }
@@ -205,10 +205,11 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
       if (active) {
         for (int h = 0; h < 2; ++h) {
           if (cw[h] < 0) continue;
-          if (run) ++itv[h];
+          if (run) itv += h ? 0x10000u : 1u;
+          const int ith = (int)(h ? itv >> 16 : itv & 0xFFFFu);
           const bool pass = run && s_crc[2 * g + h] == 0u;
-          if (pass || itv[h] >= p.max_it) {
-            mixed_emit(p, lq, zx, Zc, cw[h], h, pass ? 0 : 1, itv[h]);
+          if (pass || ith >= p.max_it) {
+            mixed_emit(p, lq, zx, Zc, cw[h], h, pass ? 0 : 1, ith);
             refill[h] = true;
           }
         }
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
         for (int h = 0; h < 2; ++h) {
           if (!refill[h]) continue;
           cw[h] = s_cw[2 * g + h];
-          itv[h] = 0;
+          itv &= h ? 0x0000FFFFu : 0xFFFF0000u;
           if (cw[h] >= 0) {
             recover_half(p, s_g, cw[h], h, lq, zx);
             fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
