@@ -378,10 +378,12 @@ __global__ void __launch_bounds__(kThreadsTarget, sizeof(Real) > 4 ? 1 : 2)
       for (int row = 0; row < p.R; ++row) {
         if (valid) {
           const int e0 = p.row_off[row], deg = p.row_off[row + 1] - e0;
-          if (old_msg && row + 1 < p.R) {   // the next row's checkpointed messages
+          if (old_msg && row + 1 < p.R) {   // the next row's checkpointed messages (all four planes)
             MsgBlock<Real> m(old_msg, row + 1, p.msg_words, p.Zc);
             prefetch_l2(m.mag + zx);
+            prefetch_l2(m.mag + p.Zc + zx);
             prefetch_l2(m.bits + zx);
+            prefetch_l2(m.bits + p.Zc + zx);
           }
           const Real alpha = alpha_t[t * p.R + row], beta = beta_t[t * p.R + row];
           NRLDPC_TRAIN_DISPATCH(train_row_fwd, Real, deg, p, lq, (uint32_t)zx, e0, row, alpha, beta, old_msg,
