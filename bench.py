@@ -60,11 +60,13 @@ def algorithmic_bytes(iters: np.ndarray, E: int = E, fp: bool = False) -> float:
 
 
 def synthetic_llrs(n: int, seed: int) -> np.ndarray:
-    rng = np.random.default_rng(seed)
+    """n blocks of E int16 LLRs; every chunk of 256 blocks has its own generator
+    (seed, chunk), so any process can regenerate any slice of the same blocks."""
     sigma = np.sqrt(0.5 / (10 ** (EBN0_DB / 10)))
     out = np.empty((n, E), dtype=np.int16)
     for s in range(0, n, 256):
         e = min(n, s + 256)
+        rng = np.random.default_rng([seed, s // 256])
         x = 1.0 - 2.0 * rng.integers(0, 2, size=(e - s, E)).astype(np.float32)
         y = x + np.float32(sigma) * rng.standard_normal((e - s, E), dtype=np.float32)
         out[s:e] = np.clip(np.rint(y * np.float32(256.0 / sigma ** 2)), -10000, 10000).astype(np.int16)
@@ -139,49 +141,149 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# ----------------------------------------------------------------------------- CPU baseline
-def _cpu_worker(args):
-    kind, n, seed = args
+# ----------------------------------------------------------------------------- reference decode of the same blocks
+def _ref_check_worker(job):
+    """Decode blocks [lo, hi) of `folder/llr.npy` on one host core with the
+    reference C library built from its sources ("reference") or this repo's C
+    restatement ("port"), timing only the decode calls, and compare every block
+    with the GPU results saved beside the LLRs (when present)."""
+    kind, folder, lo, hi, cfg_t, row = job
     sys.path.insert(0, REPO)
-    llr = synthetic_llrs(n, seed)
+    from oracle.oracle import Oracle, RefLib, dec_cfg, in_config
+
+    cfg, dcfg = in_config(*cfg_t), dec_cfg(row)
+    fp = row[0] in (0, 4)
+    llr = np.load(os.path.join(folder, "llr.npy"), mmap_mode="r")
+    gpu = None
+    if os.path.exists(os.path.join(folder, "status.npy")):
+        gpu = {k: np.load(os.path.join(folder, k + ".npy"), mmap_mode="r")
+               for k in ("status", "hardbits", "iterations", "app")}
     if kind == "reference":
-        from oracle.oracle import RefLib, dec_cfg, in_config
-
         ref = RefLib()
-        cfg, d = in_config(*CFG), dec_cfg(ROW)
-        t0 = time.perf_counter()
-        for i in range(n):
-            ref.decode(llr[i], cfg, d)
-        return time.perf_counter() - t0
-    from oracle.oracle import Oracle, dec_cfg, in_config
+        rc, p = ref.gen(cfg)
+        acc = {1: ref.lib.ref_fixed_lq, 2: ref.lib.ref_neural_lq, 3: ref.lib.ref_degree_lq,
+               0: ref.lib.ref_float_lq, 4: ref.lib.ref_float_lq}[row[0]]
+        fn = ref.lib.c_ldpc_5g_decode
+    else:
+        orc = Oracle()
+        rc, p = orc.derive(cfg)
+    assert rc == 0
+    n_app = p.N + 2 * p.Zc
+    nb = (p.B + 7) // 8
+    bits = np.zeros(nb, dtype=np.uint8)
+    lq = np.zeros(n_app, dtype=np.float32 if fp else np.int16)
+    it = ctypes.c_int32(0)
+    r = {"t": 0.0, "n": hi - lo, "converged": 0, "status": 0, "hardbits_blocks": 0, "hardbits_bits": 0,
+         "iterations": 0, "iterations_compared": 0, "app_blocks": 0, "llr_beyond_1e-4": 0, "llr_sign": 0,
+         "llr_max_abs": 0.0, "llr_values": 0}
+    for i in range(lo, hi):
+        x = np.ascontiguousarray(llr[i], dtype=np.int16)
+        bits[:] = 0
+        if kind == "reference":
+            t0 = time.perf_counter()
+            st = fn(x.ctypes.data, bits.ctypes.data, ctypes.byref(cfg), ctypes.byref(dcfg))
+            r["t"] += time.perf_counter() - t0
+            lq = np.ctypeslib.as_array(acc(), shape=(n_app,))
+            its = row[1] if st == 1 else None      # the reference does not report its iteration count
+        else:
+            t0 = time.perf_counter()
+            st = orc.lib.orc_decode(x.ctypes.data, bits.ctypes.data, ctypes.byref(cfg), ctypes.byref(dcfg),
+                                    orc.harq.ctypes.data, lq.ctypes.data, ctypes.byref(it))
+            r["t"] += time.perf_counter() - t0
+            its = int(it.value)
+        r["converged"] += int(st == 0)
+        if gpu is None:
+            continue
+        r["status"] += int(int(gpu["status"][i]) != st)
+        diff = int(np.unpackbits(np.bitwise_xor(np.asarray(gpu["hardbits"][i][:nb]), bits)).sum())
+        r["hardbits_blocks"] += int(diff > 0)
+        r["hardbits_bits"] += diff
+        if its is not None:
+            r["iterations_compared"] += 1
+            r["iterations"] += int(int(gpu["iterations"][i]) != its)
+        g = np.asarray(gpu["app"][i][:n_app])
+        if fp:
+            d = np.abs(g.astype(np.float64) - lq.astype(np.float64))
+            r["llr_values"] += n_app
+            r["llr_beyond_1e-4"] += int(np.sum(d > 1e-4 * np.abs(lq) + 1e-6))
+            r["llr_sign"] += int(np.sum(np.signbit(g) != np.signbit(lq)))
+            r["llr_max_abs"] = max(r["llr_max_abs"], float(d.max()))
+            r["app_blocks"] += int(not np.array_equal(g, lq))
+        else:
+            r["app_blocks"] += int(not np.array_equal(g, lq))
+    return r
 
-    orc = Oracle()
-    t0 = time.perf_counter()
-    orc.decode_many(llr, in_config(*CFG), dec_cfg(ROW))
-    return time.perf_counter() - t0
 
-
-def cpu_baseline(per_proc: int = 0, procs: int = 0) -> dict:
-    """The reference's C decoder (built from its sources into oracle/_ref) if
-    present, else this repo's C restatement, one process per host core (the
-    decoders keep state in file-static buffers, so one process each)."""
+def reference_decode(host_llr, cfg, row, gpu=None, procs: int = 0, a_bits: int = A_BITS) -> dict:
+    """Decode every block of `host_llr` with the reference C decoder (built from
+    its sources into oracle/_ref; else the oracle port) in one process per host
+    core (the reference decoders keep state in file-static buffers), timing the
+    decode calls.  With `gpu` (numpy status, hardbits, iterations, app of the
+    same blocks) every block is compared field by field."""
     import multiprocessing as mp
+    import shutil
+    import tempfile
 
     from oracle.oracle import REF_SO
 
     kind = "reference" if os.path.exists(REF_SO) else "port"
-    procs = procs or len(os.sched_getaffinity(0)) or 1
-    per_proc = per_proc or 768   # about 10 s of decoding per process on the B200 hosts
-    ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    with ctx.Pool(procs) as pool:
-        times = pool.map(_cpu_worker, [(kind, per_proc, 1000 + r) for r in range(procs)])
-    wall = time.perf_counter() - t0
-    slowest = max(times)
-    gbps = procs * per_proc * A_BITS / slowest / 1e9
-    return {"value": gbps, "unit": "Gbit/s", "cores": procs, "kind": kind,
-            "sample": (f"{procs} processes x {per_proc} code blocks of the same workload (noisy, 8 iterations run), "
-                       f"sum of A bits / slowest process time ({slowest:.1f} s; pool wall {wall:.1f} s)")}
+    n = host_llr.shape[0]
+    procs = max(1, min(procs or len(os.sched_getaffinity(0)) or 1, n))
+    folder = tempfile.mkdtemp(prefix="ldpc_refcheck_")
+    try:
+        np.save(os.path.join(folder, "llr.npy"), host_llr)
+        if gpu is not None:
+            for k in ("status", "hardbits", "iterations", "app"):
+                np.save(os.path.join(folder, k + ".npy"), gpu[k])
+        bounds = [(r * n // procs, (r + 1) * n // procs) for r in range(procs)]
+        jobs = [(kind, folder, lo, hi, tuple(cfg), list(row)) for lo, hi in bounds]
+        t0 = time.perf_counter()
+        with mp.get_context("spawn").Pool(procs) as pool:
+            parts = pool.map(_ref_check_worker, jobs)
+        wall = time.perf_counter() - t0
+    finally:
+        shutil.rmtree(folder, ignore_errors=True)
+    slowest = max(p["t"] for p in parts)
+    tot = {k: sum(p[k] for p in parts) for k in parts[0] if k not in ("t", "llr_max_abs")}
+    out = {"kind": kind, "cores": procs, "blocks": n, "slowest_s": slowest, "wall_s": wall,
+           "gbps": n * a_bits / slowest / 1e9, "converged": tot["converged"]}
+    if gpu is not None:
+        fp = row[0] in (0, 4)
+        par = {"blocks": n, "against": ("reference c_lib built from its sources (oracle/_ref), c_ldpc_5g_decode"
+                                        if kind == "reference" else "C restatement of the reference (oracle port)"),
+               "status_mismatches": tot["status"], "hardbit_block_mismatches": tot["hardbits_blocks"],
+               "hardbit_mismatches": tot["hardbits_bits"],
+               "iteration_mismatches": tot["iterations"], "iterations_compared": tot["iterations_compared"],
+               "final_llr_block_mismatches": tot["app_blocks"]}
+        if fp:
+            par.update({"llr_values": tot["llr_values"], "llr_beyond_1e-4_rel": tot["llr_beyond_1e-4"],
+                        "llr_beyond_1e-4_rate": tot["llr_beyond_1e-4"] / max(1, tot["llr_values"]),
+                        "llr_sign_mismatches": tot["llr_sign"],
+                        "llr_max_abs_diff": max(p["llr_max_abs"] for p in parts),
+                        "hardbit_block_mismatch_rate": tot["hardbits_blocks"] / n})
+            par["mismatches"] = tot["status"] + tot["hardbits_blocks"] + tot["iterations"]
+            par["fields"] = "status, hard bits, iterations (exact); final float LLRs (statistics)"
+        else:
+            par["mismatches"] = tot["status"] + tot["hardbits_blocks"] + tot["iterations"] + tot["app_blocks"]
+            par["fields"] = "status, hard bits, iterations, final int16 LLRs (all exact)"
+        if kind == "reference":
+            par["iterations_note"] = ("the reference reports no iteration count: compared where it is implied "
+                                      "(status 1 = max_iterations); the final LLRs pin the exit iteration")
+        out["parity"] = par
+    return out
+
+
+def cpu_baseline_from(ref: dict, what: str) -> dict:
+    return {"value": ref["gbps"], "unit": "Gbit/s", "cores": ref["cores"], "kind": ref["kind"],
+            "sample": (f"{what}: {ref['blocks']} code blocks split over {ref['cores']} processes (one per host "
+                       f"core), sum of A bits / slowest process's decode time ({ref['slowest_s']:.1f} s; "
+                       f"pool wall {ref['wall_s']:.1f} s)")}
+
+
+def gpu_results(res, n_app=None) -> dict:
+    """Host copies of a DecodeResult for the reference comparison."""
+    return {"status": res.status.cpu().numpy(), "hardbits": res.hardbits.cpu().numpy(),
+            "iterations": res.iterations.cpu().numpy(), "app": res.app.cpu().numpy()}
 
 
 # ----------------------------------------------------------------------------- GPU arm
@@ -191,7 +293,6 @@ def run_gpu(args, rank, world, local_rank):
     from deeplearning_5g_ldpc_decoder_b200.shard import max_over_ranks, sum_over_ranks
 
     from deeplearning_5g_ldpc_decoder_b200 import capi, ldpc_decode
-    from deeplearning_5g_ldpc_decoder_b200.capi import make_decoder_config, make_in_config
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -245,20 +346,39 @@ def run_gpu(args, rank, world, local_rank):
     status = out.status.cpu().numpy()
     ms_step = max_over_ranks(total_ms / args.steps, dist, dev)
     info_bits = sum_over_ranks(n_cw * A_BITS, dist, dev)
+    # the blocks of the timed step once more with their final beliefs (untimed), for the reference comparison
+    checks = []
+    do_parity = rank == 0 and world == 1 and not args.no_parity
+    if do_parity:
+        chk = ldpc_decode(d_llr, CFG, row, return_app=True)
+        torch.cuda.synchronize(dev)
+        assert torch.equal(chk.hardbits, out.hardbits) and torch.equal(chk.status, out.status) \
+            and torch.equal(chk.iterations, out.iterations), "the final-belief launch differs from the timed one"
+        checks.append(("main", host_llr, CFG, row, gpu_results(chk)))
+        del chk
 
     # ---- realistic inputs: device-encoded code blocks through the 256QAM channel
     # near the 1e-2 BLER point; CRC early termination as in the reference ----
     early = None
     variants = None
     if not args.no_e2e:
-        early = run_early_exit(args, n_cw, dev, stream, barrier, dist, torch)
-        variants = run_config2_variants(args, n_cw, dev, stream, barrier, dist, torch)
+        early = run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, checks=checks if do_parity else None)
+        variants = run_config2_variants(args, n_cw, dev, stream, barrier, dist, torch,
+                                        checks=checks if do_parity else None)
 
     # ---- end to end through the host-buffer C ABI (pinned memory) ----
     if args.no_e2e:
         e2e_ms = float("nan")
     else:
         e2e_ms = run_e2e(args, lib, host_llr, out, stream, barrier, dist, dev, iters, torch)
+
+    per_call = run_per_call(args) if (rank == 0 and world == 1 and not args.no_e2e) else None
+
+    # ---- every block of every leg decoded again by the reference C decoder on the host cores ----
+    refs = {}
+    for name, llr_h, cfg, row_c, gpu in checks:
+        refs[name] = reference_decode(llr_h, cfg, row_c, gpu=gpu, procs=args.cpu_procs,
+                                      a_bits=cfg[1])
     result = None
     if rank == 0:
         value = info_bits / (ms_step * 1e-3) / 1e9
@@ -299,15 +419,30 @@ def run_gpu(args, rank, world, local_rank):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "traffic": (round(traffic_cw * n_cw) if traffic_cw else None),
+                         "traffic_source": ("profile constant, not measured in this run: ncu dram__bytes_read.sum + "
+                                            "dram__bytes_write.sum per block of the committed capture "
+                                            "(profiles/fixed_pair_kernel_bg1_zc384.md) x blocks per launch"
+                                            if traffic_cw else "no ncu capture of this decoder's launch"),
                          "algorithmic_bytes_per_launch": alg, "kernel_ms": round(mean_launch_ms, 4),
                          "io_bytes_per_launch": float((2 * E + (B_BITS + 7) // 8 + 4) * n_cw)},
             "iterations_executed_mean": float(np.mean(iters)),
             "converged": int(np.sum(status == 0)),
             "early_exit": early,
             "config2_variants": variants,
+            "per_call": per_call,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
+        if "main" in refs:
+            result["parity"] = refs["main"]["parity"]
+            result["cpu_baseline"] = cpu_baseline_from(
+                refs["main"], "the timed step's own blocks (seed 0, noisy, all 8 iterations run)")
+        for leg in (early, *(variants or {}).values()):
+            if leg is not None and leg.get("_check") in refs:
+                ref = refs[leg.pop("_check")]
+                leg["parity"] = ref["parity"]
+                leg["reference_cpu_gbps"] = round(ref["gbps"], 6)
+                leg["reference_converged"] = ref["converged"]
         if args.no_e2e:
             result["e2e"] = None
     if dist is not None:
@@ -335,9 +470,11 @@ def _esn0_for_bler(cfg, row, Qm, target, dev, torch, n_cw: int = 2048, lo: float
     return round(0.5 * (lo + hi), 2)
 
 
-def run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, cfg=None, row=None, esn0=None):
+def run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, cfg=None, row=None, esn0=None, checks=None,
+                   name="early_exit"):
     """Realistic inputs: device-encoded payloads through the 256QAM channel at the
-    given Es/N0, CRC early termination as in the reference."""
+    given Es/N0, CRC early termination as in the reference.  With `checks`, the
+    leg's LLRs and final beliefs are queued for the reference comparison."""
     from deeplearning_5g_ldpc_decoder_b200.shard import max_over_ranks
     from deeplearning_5g_ldpc_decoder_b200 import channel_llrs, ldpc_decode, ldpc_encode
 
@@ -363,23 +500,33 @@ def run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, cfg=None, row=
     iters = out.iterations.cpu().numpy()
     world = dist.get_world_size() if dist is not None else 1
     fp = row[0] in (0, 4)
-    return {"value": round(n_cw * A_BITS * world / (ms * 1e-3) / 1e9, 4), "unit": "Gbit/s", "ms_per_step": round(ms, 4),
-            "iterations_executed_mean": float(np.mean(iters)), "bler": float(1.0 - ok.float().mean().item()),
-            "roofline_achieved_gbs": round(algorithmic_bytes(iters, E=cfg[3], fp=fp) / (ms * 1e-3) / 1e9, 1),
-            "inputs": f"device-encoded random payloads, E={cfg[3]}, 256QAM AWGN at Es/N0 {esn0} dB, max-log LLRs "
-                      "quantised like the reference channel",
-            "decoder": {0: "algo 0 float BP", 1: "algo 1 int16 min-sum", 4: "algo 4 float min-sum"}.get(row[0], str(row[0]))}
+    leg = {"value": round(n_cw * A_BITS * world / (ms * 1e-3) / 1e9, 4), "unit": "Gbit/s", "ms_per_step": round(ms, 4),
+           "iterations_executed_mean": float(np.mean(iters)), "bler": float(1.0 - ok.float().mean().item()),
+           "roofline_achieved_gbs": round(algorithmic_bytes(iters, E=cfg[3], fp=fp) / (ms * 1e-3) / 1e9, 1),
+           "inputs": f"device-encoded random payloads, E={cfg[3]}, 256QAM AWGN at Es/N0 {esn0} dB, max-log LLRs "
+                     "quantised like the reference channel",
+           "decoder": {0: "algo 0 float BP", 1: "algo 1 int16 min-sum", 4: "algo 4 float min-sum"}.get(row[0], str(row[0]))}
+    if checks is not None:
+        chk = ldpc_decode(llr, cfg, row, return_app=True)
+        torch.cuda.synchronize(dev)
+        assert torch.equal(chk.hardbits, out.hardbits) and torch.equal(chk.status, out.status)
+        checks.append((name, llr.cpu().numpy(), cfg, row, gpu_results(chk)))
+        leg["_check"] = name
+        del chk
+    return leg
 
 
-def run_config2_variants(args, n_cw, dev, stream, barrier, dist, torch):
+def run_config2_variants(args, n_cw, dev, stream, barrier, dist, torch, checks=None):
     """The other legs of the large single-size batch: E=9600 (rate 0.88) with algo 1,
     and algo 0 (float BP) at E=25344, each at its measured ~1e-2 BLER point."""
     cfg88 = (1, 8424, 1, 9600, 0, 8, 0)
     row_bp = [0, 8, 22936, 0, 1280, 32767, -32767]
     esn0_88 = _esn0_for_bler(cfg88, ROW, 8, 0.01, dev, torch)
     esn0_bp = _esn0_for_bler(CFG, row_bp, 8, 0.01, dev, torch, n_cw=1024, lo=5.0, hi=15.0)
-    out = {"E9600_algo1": run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, cfg88, ROW, esn0_88),
-           "E25344_algo0_bp": run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, CFG, row_bp, esn0_bp)}
+    out = {"E9600_algo1": run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, cfg88, ROW, esn0_88,
+                                         checks=checks, name="E9600_algo1"),
+           "E25344_algo0_bp": run_early_exit(args, n_cw, dev, stream, barrier, dist, torch, CFG, row_bp, esn0_bp,
+                                             checks=checks, name="E25344_algo0_bp")}
     return out
 
 
@@ -418,6 +565,75 @@ def run_e2e(args, lib, host_llr, out, stream, barrier, dist, dev, iters, torch):
     assert np.array_equal(pin_it.numpy(), iters) and np.array_equal(pin_bits.numpy(), out.hardbits.cpu().numpy())
 
     return e2e_ms
+
+
+PER_CALL_CASES = [(1, 488, 1, 1536, 0, 1, 0), (1, 1024, 0, 3072, 0, 1, 0), (1, 2400, 2, 8192, 0, 1, 0),
+                  (1, 4072, 1, 16384, 0, 1, 0), (2, 176, 1, 512, 0, 1, 0), (2, 640, 3, 2048, 0, 1, 0),
+                  (2, 1200, 0, 4096, 0, 1, 0), (2, 2400, 2, 8192, 0, 1, 0)]
+PER_CALL_ROW = [1, 32, 22936, 0, 1280, 32767, -32767]
+
+
+def run_per_call(args, warmup: int = 2, calls: int = 20) -> dict:
+    """Latency of one drop-in call (cuda_ldpc_5g_decode with host buffers: copy in,
+    decode, copy out, return) on the 8 cases and with the protocol of the
+    reference's CUDA decoder test (CUDA/test_ldpc_5g_decoder.cu:318-327: BPSK at
+    0 dB, algo 1, 32 iterations; :271-309: 2 warm-up then 20 timed calls, the
+    hard-bit buffer cleared before each).  Inputs come from this library's own
+    encoder and channel (cuda_ldpc_5g_encode, tx_rx_process).  The reference C
+    decoder, timed on the same LLRs by the same protocol on one host core, is
+    the CPU side; hard bits and status must agree."""
+    from deeplearning_5g_ldpc_decoder_b200 import capi
+
+    lib = capi.load_library()
+    ref = None
+    if not args.no_parity:
+        from oracle.oracle import REF_SO, RefLib
+
+        if os.path.exists(REF_SO):
+            ref = RefLib()
+    dcfg = capi.make_decoder_config(PER_CALL_ROW)
+    rng = np.random.default_rng(2000)
+    cases = []
+    for k, c in enumerate(PER_CALL_CASES):
+        icfg = capi.make_in_config(*c)
+        p = capi.gen_ldpc_parameters(icfg)
+        info = np.zeros(1056, dtype=np.uint8)
+        info[: c[1] // 8] = rng.integers(0, 256, c[1] // 8, dtype=np.uint8)
+        rm = np.zeros((c[3] + 7) // 8 + 8, dtype=np.uint8)
+        assert lib.cuda_ldpc_5g_encode(info.ctypes.data, rm.ctypes.data, ctypes.byref(icfg)) == 0
+        lib.nrldpc_channel_seed(1000 + c[1] + c[3] + c[5] * 17)
+        llr = np.zeros(c[3], dtype=np.int16)
+        assert lib.tx_rx_process(rm.ctypes.data, c[3], c[5], ctypes.c_float(0.0), llr.ctypes.data) == 0
+        nb = (p.B + 7) // 8
+        bits = np.zeros(nb, dtype=np.uint8)
+
+        def timed(fn, ic, dc):
+            for _ in range(warmup):
+                bits[:] = 0
+                st = fn(llr.ctypes.data, bits.ctypes.data, ctypes.byref(ic), ctypes.byref(dc))
+            t0 = time.perf_counter()
+            for _ in range(calls):
+                bits[:] = 0
+                st = fn(llr.ctypes.data, bits.ctypes.data, ctypes.byref(ic), ctypes.byref(dc))
+            return (time.perf_counter() - t0) * 1e3 / calls, int(st), bits.copy()
+
+        ms, st, got = timed(lib.cuda_ldpc_5g_decode, icfg, dcfg)
+        ok = st == 0 and np.array_equal(got[: c[1] // 8], info[: c[1] // 8])
+        leg = {"case": list(c), "Zc": int(p.Zc), "ms_per_call": round(ms, 4), "status": st, "payload_ok": bool(ok)}
+        if ref is not None:
+            from oracle.oracle import dec_cfg, in_config
+
+            rms, rst, rbits = timed(ref.lib.c_ldpc_5g_decode, in_config(*c), dec_cfg(PER_CALL_ROW))
+            leg.update({"reference_c_ms_per_call": round(rms, 4), "reference_status": rst,
+                        "same_result": bool(rst == st and np.array_equal(rbits, got)),
+                        "speedup": round(rms / ms, 2)})
+        cases.append(leg)
+    head = cases[3]
+    return {"protocol": f"{warmup} warm-up + {calls} timed calls per case, host buffers, synchronous return "
+                        "(CUDA/test_ldpc_5g_decoder.cu:271-309); BPSK at 0 dB, algo 1, 32 iterations",
+            "headline_case": "cases[3] = (1, 4072, 1, 16384, 0, 1, 0), the case the reference test profiles",
+            "ms_per_call": head["ms_per_call"], "reference_c_ms_per_call": head.get("reference_c_ms_per_call"),
+            "cases": cases}
 
 
 def run_mixed(args):
@@ -708,7 +924,7 @@ def run_train(args):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     base = None
-    if not args.no_cpu_baseline:
+    if not args.no_parity:
         base = _train_cpu_baseline(TRAIN_CONFIGS["bg2_zc64"], T)
     legs = {}
     for name, cfg in TRAIN_CONFIGS.items():
@@ -776,8 +992,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-per-proc", type=int, default=0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-procs", type=int, default=0, help="host processes of the reference decode (0: all cores)")
+    ap.add_argument("--no-parity", "--no-cpu-baseline", dest="no_parity", action="store_true",
+                    help="skip the reference decode of the same blocks (parity and CPU baseline)")
     ap.add_argument("--n-cw", type=int, default=N_CW, help="code blocks per step (profiling runs use fewer)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--algo", type=int, default=1, choices=[0, 1, 2, 3, 4],
@@ -787,6 +1004,11 @@ def main():
                     help="mixed: 32768 blocks over all 51 lifting sizes, BG1 60 %%, rate U[0.2, 0.92], Qm 2-8; "
                          "train: learned min-sum forward+backward, batch 4096, 10 iterations")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # asked for N GPUs outside a launcher: start one rank per GPU here
+        from deeplearning_5g_ldpc_decoder_b200.shard import launch_ranks
+
+        sys.exit(launch_ranks(args.gpus, os.path.abspath(__file__), sys.argv[1:], timeout_s=1800))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -794,13 +1016,17 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        base = cpu_baseline(per_proc=args.cpu_per_proc or 0)
+        llr = synthetic_llrs(args.n_cw, seed=0)
+        ref = reference_decode(llr, CFG, ROW, procs=args.cpu_procs)
+        base = cpu_baseline_from(ref, "the GPU arm's rank-0 step (seed 0, noisy, all 8 iterations run)")
         line = {
             "metric": METRIC, "value": round(base["value"], 6), "unit": "Gbit/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int16", "impl": "reference",
-            "data": "same synthetic LLRs as the GPU arm (noisy, 8 iterations run)",
-            "config": {"workload": WORKLOAD, "parallelism": "one process per host core"},
+            "data": (f"the GPU arm's own rank-0 LLRs: all {args.n_cw} blocks of synthetic_llrs(seed 0), random bits "
+                     "on BPSK/AWGN at Eb/N0 0.9 dB (noisy, all 8 iterations run)"),
+            "config": {"workload": WORKLOAD.replace("8192", str(args.n_cw)),
+                       "parallelism": "one process per host core"},
             "cpu_baseline": base,
             "e2e": {"value": round(base["value"], 6), "unit": "Gbit/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -824,13 +1050,11 @@ def main():
         print(json.dumps(run_serve(args)), flush=True)
         return
 
-    # The CPU baseline pool is spawned before any GPU work.
-    base = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(per_proc=args.cpu_per_proc or 0)
+    if world > 1:
+        os.environ.setdefault("NCCL_DEBUG", "INFO")     # the communicator's rank count shows in the log
     result = run_gpu(args, rank, world, local_rank)
     if rank == 0:
-        result["cpu_baseline"] = base
+        result.setdefault("cpu_baseline", None)
         print(json.dumps(result), flush=True)
 
 

@@ -32,4 +32,9 @@ def __getattr__(name):
         from . import decoder
 
         return getattr(decoder, name)
+    if name == "ops":
+        # importing it registers torch.ops.nrldpc.ldpc_decode
+        import importlib
+
+        return importlib.import_module(".ops", __name__)
     raise AttributeError(name)

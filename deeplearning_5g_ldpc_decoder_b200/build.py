@@ -22,6 +22,9 @@ CSRC = os.path.join(PKG_DIR, "csrc")
 INCLUDE = os.path.join(REPO_DIR, "include")
 LIB_NAME = "libnrldpc_b200.so"
 LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
+# Debug build: the same sources with device-side index checks on every gather
+# and scatter of the decode kernels (-DNRLDPC_BOUNDS_CHECK); never on the product path.
+DEBUG_LIB_PATH = os.path.join(PKG_DIR, "libnrldpc_b200_debug.so")
 
 SOURCES = [
     "nrldpc_api.cu",
@@ -40,6 +43,7 @@ HEADERS = [
     "nrldpc_internal.h",
     "nrldpc_decode_common.cuh",
     "nrldpc_fixed_row.cuh",
+    "nrldpc_bounds.cuh",
     "nrldpc_tb.cuh",
     "nr_base_graphs.inc",
 ]
@@ -61,17 +65,19 @@ def _inputs():
     return files
 
 
-def up_to_date() -> bool:
-    if not os.path.exists(LIB_PATH):
+def up_to_date(path: str = LIB_PATH) -> bool:
+    if not os.path.exists(path):
         return False
-    t = os.path.getmtime(LIB_PATH)
+    t = os.path.getmtime(path)
     return all(os.path.getmtime(f) <= t for f in _inputs())
 
 
-def build_library(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
-    """Compile the library if any input is newer than it; return its path."""
-    if not force and up_to_date():
-        return LIB_PATH
+def build_library(force: bool = False, verbose: bool = False, extra_flags=None, debug: bool = False) -> str:
+    """Compile the library (or, with debug, the bounds-checked debug library) if
+    any input is newer than it; return its path."""
+    out = DEBUG_LIB_PATH if debug else LIB_PATH
+    if not force and up_to_date(out):
+        return out
     cmd = [
         nvcc_path(),
         *ARCH_FLAGS,
@@ -88,8 +94,10 @@ def build_library(force: bool = False, verbose: bool = False, extra_flags=None) 
         cmd += ["-Xptxas", "-v"]
     if extra_flags:
         cmd += list(extra_flags)
+    if debug:
+        cmd += ["-DNRLDPC_BOUNDS_CHECK"]
     cmd += [os.path.join(CSRC, s) for s in SOURCES]
-    tmp = LIB_PATH + ".tmp"
+    tmp = out + ".tmp"
     cmd += ["-o", tmp, "-lpthread", "-ldl", "-lrt"]
     proc = subprocess.run(cmd, cwd=PKG_DIR, capture_output=True, text=True)
     if proc.returncode != 0:
@@ -98,16 +106,17 @@ def build_library(force: bool = False, verbose: bool = False, extra_flags=None) 
         raise RuntimeError(f"nvcc failed with exit code {proc.returncode}")
     if verbose:
         sys.stderr.write(proc.stderr)
-    os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+    os.replace(tmp, out)
+    return out
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--debug", action="store_true", help="the bounds-checked debug library")
     args = ap.parse_args()
-    print(build_library(force=args.force, verbose=args.verbose))
+    print(build_library(force=args.force, verbose=args.verbose, debug=args.debug))
 
 
 if __name__ == "__main__":

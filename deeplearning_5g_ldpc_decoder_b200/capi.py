@@ -144,6 +144,7 @@ EXPORTED_SYMBOLS = (
     "nrldpc_serve_run",
     "nrldpc_kernel_launch_count",
     "nrldpc_version",
+    "nrldpc_bounds_check_status",
 )
 
 
@@ -241,6 +242,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nrldpc_kernel_launch_count.restype = i64
     lib.nrldpc_version.argtypes = []
     lib.nrldpc_version.restype = ctypes.c_char_p
+    lib.nrldpc_bounds_check_status.argtypes = [vp, i32]
+    lib.nrldpc_bounds_check_status.restype = i32
 
 
 def gen_ldpc_parameters(cfg: LdpcInConfig, lib=None) -> LdpcConfig:

@@ -14,6 +14,7 @@
 
 #include <math.h>
 
+#include "nrldpc_bounds.cuh"
 #include "nrldpc_internal.h"
 
 namespace nrldpc {
@@ -817,7 +818,23 @@ int32_t nrldpc_set_degree_alpha(const int16_t* degree_alpha_values) {
 
 int64_t nrldpc_kernel_launch_count(void) { return g_launches.load(); }
 
-const char* nrldpc_version(void) { return "nrldpc-b200 0.1.0 (sm_100a)"; }
+const char* nrldpc_version(void) {
+  return kBoundsChecked ? "nrldpc-b200 0.1.0 (sm_100a, bounds-checked debug build)" : "nrldpc-b200 0.1.0 (sm_100a)";
+}
+
+int32_t nrldpc_bounds_check_status(uint32_t* out, int32_t reset) {
+  if (!out) return NRLDPC_ERR_ARG;
+  out[0] = out[1] = out[2] = out[3] = 0u;
+  if (!kBoundsChecked) return 0;
+  // first record among the kernels' translation units (fixed-point, float, mixed)
+  int (*readers[3])(uint32_t*, bool) = {bounds_read_fixed, bounds_read_float, bounds_read_mixed};
+  for (auto rd : readers) {
+    uint32_t r[4];
+    if (rd(r, reset != 0) != 0) return NRLDPC_ERR_CUDA;
+    if (out[0] == 0u && r[0] != 0u) memcpy(out, r, sizeof(r));
+  }
+  return 1;
+}
 
 int32_t nrldpc_encode_batch(const uint8_t* d_info, int64_t info_stride, int32_t num_cw,
                             const ldpc_in_config_t* inconfig, uint8_t* d_rm, int64_t rm_stride, void* stream) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "nrldpc_bounds.cuh"
 #include "nrldpc_internal.h"
 
 namespace nrldpc {
@@ -34,14 +35,15 @@ __device__ __forceinline__ int32_t recover_position(const DecodeParams& p, const
   for (int k = kf; k < p.E; k += p.Nv) {
     const int b = k / p.symbols;
     const int sidx = k - b * p.symbols;
-    s += __ldg(in + (int64_t)sidx * p.Qm + b);
+    const int64_t idx = (int64_t)sidx * p.Qm + b;
+    if (NRLDPC_INBOUNDS(idx, p.E, kBoundsLlr)) s += __ldg(in + idx);
   }
   return s;
 }
 
 // CRC remainder contribution of one hard bit: T[B-1-i] if bit i is set.
 __device__ __forceinline__ uint32_t crc_term(const DecodeParams& p, int i) {
-  return __ldg(p.crc_tab + (p.B - 1 - i));
+  return NRLDPC_INBOUNDS(p.B - 1 - i, kMaxB, kBoundsCrc) ? __ldg(p.crc_tab + (p.B - 1 - i)) : 0u;
 }
 
 }  // namespace nrldpc

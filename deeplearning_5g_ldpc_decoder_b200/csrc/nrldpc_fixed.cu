@@ -165,10 +165,16 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
   const bool active = g < p.G;
   uint32_t* lq = s_lq + (active ? g : 0) * p.lq_len;
   uint32_t* scratch = p.scratch + (int64_t)blockIdx.x * p.scratch_words;
+  // debug build: every message word of the CTA (planes of kThreadsTarget words,
+  // ending at lr_off[R]) lies inside its scratch
+  if (!NRLDPC_INBOUNDS(p.lr_off[p.R] - 1u, p.scratch_words, kBoundsScratch) ||
+      !NRLDPC_INBOUNDS(blockDim.x - 1u, kThreadsTarget, kBoundsScratch))
+    return;
   const int Bp = (p.B + 31) & ~31;
   const uint32_t zx4 = 4u * (uint32_t)zx;
   const uint32_t zxm4 = zx4 - 4u * (uint32_t)p.Zc;     // wraps: min(zx4+s, zxm4+s) = ((zx+V) mod Zc)*4
   const uint32_t gb4 = 4u * (uint32_t)((active ? g : 0) * p.lq_len);
+  const uint32_t lq_limit = 4u * (uint32_t)(p.G * p.lq_len);   // bytes of s_lq in use
 
   if constexpr (kRefill) {
     __shared__ int s_cw[2 * kMaxGroups];   // block in each half lane, -1 when idle
@@ -202,8 +208,8 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
           } else {
             ab0 = ab1 = p.w_inline[row];
           }
-          layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0,
-                                           (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
+          layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, lq_limit,
+                                           e0, (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
                                            (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, cur, fresh,
                                            scratch + p.lr_off[row] + tid);
         }
@@ -301,7 +307,8 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
                                                 : p.w_inline[row];
             const int32_t alpha = (int32_t)(int16_t)(ab & 0xFFFFu);
             const int32_t beta = ((int32_t)ab) >> 16;
-            layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0, alpha, beta,
+            layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, lq_limit, e0,
+                                             alpha, beta,
                                              alpha, beta, cur, it == 0 ? 0xFFFFFFFFu : 0u, scratch + p.lr_off[row] + tid);
           }
           __syncthreads();
@@ -366,6 +373,8 @@ int launch_fixed(const DecodeParams& p, int grid, int block, int smem, bool dege
   count_launch();
   return (int)cudaGetLastError();
 }
+
+int bounds_read_fixed(uint32_t* out, bool reset) { return bounds_read_tu(out, reset); }
 
 int occupancy_fixed(int block, int smem, bool degen_clip, bool refill) {
   if (degen_clip) return refill ? occupancy_fixed_t<true, true>(block, smem) : occupancy_fixed_t<true, false>(block, smem);

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "nrldpc_bounds.cuh"
 #include "nrldpc_internal.h"
 
 namespace nrldpc {
@@ -95,7 +96,7 @@ __device__ __forceinline__ RowMsg load_row_msg(const uint32_t* lrp, bool five) {
 
 template <int D, bool kDegenClip, bool kSmemEdges, typename P>
 __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__ sedges, char* __restrict__ lqs, uint32_t zx4,
-                                           uint32_t zxm4, uint32_t gb4, int e0, int32_t alpha, int32_t beta,
+                                           uint32_t zxm4, uint32_t gb4, uint32_t lq_limit, int e0, int32_t alpha, int32_t beta,
                                            int32_t alpha1, int32_t beta1, const RowMsg& old, uint32_t fresh,
                                            uint32_t* __restrict__ lrp) {
   constexpr int J = D < 16 ? D : 16;
@@ -122,6 +123,8 @@ __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__
   uint32_t sg = 0u;                       // XOR of all inputs: sign parity per half
   uint32_t m1 = 0x7FFF7FFFu, m2 = 0x7FFF7FFFu;
   uint32_t oh0 = 0u, oh1 = 0u;            // last edge reaching the running minimum
+  // debug build: the row's edge entries and (below) every belief word it touches
+  if (!NRLDPC_INBOUNDS(e0 + D - 1, kMaxNnz, kBoundsEdge)) return;
 
   // Pass 1: extrinsic inputs rel = LQ - old message (int16 wrap-around, as the
   // reference's int16 assignment at c_lib/fixedpoint_ldpc_decoder.c:203),
@@ -136,7 +139,8 @@ __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__
     }
     const uint32_t t = min(zx4 + cs.y, zxm4 + cs.y);   // ((zx + V) mod Zc) * 4
     addr[j] = t + cs.x + gb4;
-    const uint32_t q = *reinterpret_cast<const uint32_t*>(lqs + addr[j]);
+    const uint32_t q = NRLDPC_INBOUNDS(addr[j], lq_limit, kBoundsLq) ? *reinterpret_cast<const uint32_t*>(lqs + addr[j])
+                                                                      : 0u;
     uint32_t mf, mi;
     if (j < 16) {
       mf = sign_mask(xf << (J - 1 - j));
@@ -198,7 +202,7 @@ __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__
       const int32_t hi = (((int32_t)rel[j]) >> 16) + (((int32_t)lr) >> 16);
       nq = clip_half_degen(lo, p.max_llr, p.min_llr) | (clip_half_degen(hi, p.max_llr, p.min_llr) << 16);
     }
-    *reinterpret_cast<uint32_t*>(lqs + addr[j]) = nq;
+    if (NRLDPC_INBOUNDS(addr[j], lq_limit, kBoundsLq)) *reinterpret_cast<uint32_t*>(lqs + addr[j]) = nq;
   }
   if (!kDegenClip && (ovf & 0x80008000u) != 0u) {
     // Rare: some rel + msg left the int16 range.  Saturating add then clamp
@@ -214,7 +218,8 @@ __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__
         mi = sign_mask(Y << (11 - (j - 16)));
       }
       const uint32_t lr = cond_neg16x2(bsel(mi, s2, s1), mf);
-      *reinterpret_cast<uint32_t*>(lqs + addr[j]) = __vmins2(__vmaxs2(__vaddss2(rel[j], lr), minp), maxp);
+      if (NRLDPC_INBOUNDS(addr[j], lq_limit, kBoundsLq))
+        *reinterpret_cast<uint32_t*>(lqs + addr[j]) = __vmins2(__vmaxs2(__vaddss2(rel[j], lr), minp), maxp);
     }
   }
   lrp[0] = s1;
@@ -226,12 +231,12 @@ __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__
 
 template <bool kDegenClip, bool kSmemEdges, typename P>
 __device__ __forceinline__ void layer_dispatch(int deg, const P& p, const uint2* sedges, char* lqs, uint32_t zx4, uint32_t zxm4,
-                                               uint32_t gb4, int e0, int32_t alpha, int32_t beta,
+                                               uint32_t gb4, uint32_t lq_limit, int e0, int32_t alpha, int32_t beta,
                                                int32_t alpha1, int32_t beta1, const RowMsg& old, uint32_t fresh,
                                                uint32_t* lrp) {
   switch (deg) {
 #define NRLDPC_ROW(D) \
-  case D: row_update<D, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, alpha1, beta1, old, fresh, lrp); break;
+  case D: row_update<D, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, lq_limit, e0, alpha, beta, alpha1, beta1, old, fresh, lrp); break;
     NRLDPC_ROW(3)
     NRLDPC_ROW(4)
     NRLDPC_ROW(5)
@@ -241,7 +246,7 @@ __device__ __forceinline__ void layer_dispatch(int deg, const P& p, const uint2*
     NRLDPC_ROW(9)
     NRLDPC_ROW(10)
 #undef NRLDPC_ROW
-    default: row_update<19, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, e0, alpha, beta, alpha1, beta1, old, fresh, lrp); break;
+    default: row_update<19, kDegenClip, kSmemEdges>(p, sedges, lqs, zx4, zxm4, gb4, lq_limit, e0, alpha, beta, alpha1, beta1, old, fresh, lrp); break;
   }
 }
 

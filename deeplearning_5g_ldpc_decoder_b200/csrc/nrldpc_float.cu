@@ -39,6 +39,15 @@ __device__ __forceinline__ uint32_t edge_addr(const DecodeParams& p, int e, uint
   return (ed & 0xFFFFu) + t;
 }
 
+// Belief word a of the code block's LQ (debug build: a < lq_len, else the load
+// reads 0 and the store is dropped).
+__device__ __forceinline__ float ld_lq(const DecodeParams& p, const float* lq, uint32_t a) {
+  return NRLDPC_INBOUNDS(a, p.lq_len, kBoundsLq) ? lq[a] : 0.0f;
+}
+__device__ __forceinline__ void st_lq(const DecodeParams& p, float* lq, uint32_t a, float v) {
+  if (NRLDPC_INBOUNDS(a, p.lq_len, kBoundsLq)) lq[a] = v;
+}
+
 // ---------------------------------------------------------------- float min-sum
 // Stored message of a lifted check row (4 planes): new_min1, new_min2 (float
 // bits), bit j = message of edge j negated, bit j = edge j carries new_min2.
@@ -53,6 +62,7 @@ __device__ __forceinline__ void fms_row(const DecodeParams& p, float* __restrict
     xf = lrp[2 * NT];
     xi = lrp[3 * NT];
   }
+  if (!NRLDPC_INBOUNDS(e0 + D - 1, kMaxNnz, kBoundsEdge)) return;   // debug build
   float rel[D];
   uint32_t addr[D];
   float m1 = FLT_MAX, m2 = FLT_MAX;
@@ -63,7 +73,7 @@ __device__ __forceinline__ void fms_row(const DecodeParams& p, float* __restrict
     addr[j] = edge_addr(p, e0 + j, zx);
     float r = ((xi >> j) & 1u) ? n2 : n1;
     r = ((xf >> j) & 1u) ? -r : r;
-    const float v = __fsub_rn(lq[addr[j]], r);
+    const float v = __fsub_rn(ld_lq(p, lq, addr[j]), r);
     rel[j] = v;
     neg ^= (v < 0.0f);
     const float a = fabsf(v);
@@ -91,7 +101,7 @@ __device__ __forceinline__ void fms_row(const DecodeParams& p, float* __restrict
     const bool flip = (rel[j] < 0.0f) != neg;
     const float msg = flip ? -nv : nv;      // edge_sign * new_val, edge_sign = +-1
     XF |= (flip ? 1u : 0u) << j;
-    lq[addr[j]] = clipf(__fadd_rn(rel[j], msg), p.f_max, p.f_min);
+    st_lq(p, lq, addr[j], clipf(__fadd_rn(rel[j], msg), p.f_max, p.f_min));
   }
   lrp[0] = __float_as_uint(s1);
   lrp[NT] = __float_as_uint(s2);
@@ -133,6 +143,7 @@ __device__ __forceinline__ float bp_message(float prod) {
 template <int D>
 __device__ __forceinline__ void bp_row(const DecodeParams& p, float* __restrict__ lq, uint32_t zx, int e0,
                                        bool first, uint32_t* __restrict__ lrp, int NT) {
+  if (!NRLDPC_INBOUNDS(e0 + D - 1, kMaxNnz, kBoundsEdge)) return;   // debug build
   float th[D];
   int nz = 0, zidx = -1;
   float nzprod = 1.0f;
@@ -141,8 +152,8 @@ __device__ __forceinline__ void bp_row(const DecodeParams& p, float* __restrict_
   for (int j = 0; j < D; ++j) {
     const uint32_t a = edge_addr(p, e0 + j, zx);
     const float old = first ? 0.0f : __uint_as_float(lrp[j * NT]);
-    const float v = __fsub_rn(lq[a], old);
-    lq[a] = v;
+    const float v = __fsub_rn(ld_lq(p, lq, a), old);
+    st_lq(p, lq, a, v);
     if (v == 0.0f) {
       ++nz;
       zidx = j;
@@ -167,7 +178,7 @@ __device__ __forceinline__ void bp_row(const DecodeParams& p, float* __restrict_
       pre = __fmul_rn(pre, th[j]);
       const uint32_t a = edge_addr(p, e0 + j, zx);
       lrp[j * NT] = __float_as_uint(m);
-      lq[a] = __fadd_rn(lq[a], m);   // no clipping in BP (:148-150)
+      st_lq(p, lq, a, __fadd_rn(ld_lq(p, lq, a), m));   // no clipping in BP (:148-150)
     }
   } else {
     // one zero input: only its edge gets a message (the product of the
@@ -178,7 +189,7 @@ __device__ __forceinline__ void bp_row(const DecodeParams& p, float* __restrict_
       const float m = j == zidx && nz == 1 ? mz : 0.0f;
       const uint32_t a = edge_addr(p, e0 + j, zx);
       lrp[j * NT] = __float_as_uint(m);
-      lq[a] = __fadd_rn(lq[a], m);
+      st_lq(p, lq, a, __fadd_rn(ld_lq(p, lq, a), m));
     }
   }
 }
@@ -234,6 +245,9 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
   float* lq = s_lqf + (active ? g : 0) * p.lq_len;
   uint32_t* scratch = p.scratch + (int64_t)blockIdx.x * p.scratch_words;
   const int NT = p.nact;
+  // debug build: every message word of the CTA (planes of nact words, ending at
+  // lr_off[R]) lies inside its scratch
+  if (!NRLDPC_INBOUNDS(p.lr_off[p.R] - 1u, p.scratch_words, kBoundsScratch)) return;
   const int Bp = (p.B + 31) & ~31;
 
   // Work items: fixed (item += grid) or, with a queue cursor, taken from the
@@ -346,6 +360,8 @@ int launch_float_minsum(const DecodeParams& p, int grid, int block, int smem, vo
 int launch_float_bp(const DecodeParams& p, int grid, int block, int smem, void* stream) {
   return launch_impl(float_kernel<true>, p, grid, block, smem, stream);
 }
+int bounds_read_float(uint32_t* out, bool reset) { return bounds_read_tu(out, reset); }
+
 int occupancy_float_minsum(int block, int smem) { return occupancy_impl(float_kernel<false>, block, smem); }
 int occupancy_float_bp(int block, int smem) { return occupancy_impl(float_kernel<true>, block, smem); }
 

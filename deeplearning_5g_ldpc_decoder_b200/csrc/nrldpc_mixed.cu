@@ -48,7 +48,8 @@ __device__ __forceinline__ int32_t mixed_recover(const MixedGraph& g, const Mixe
   for (int k = kf; k < c.E; k += c.Nv) {
     const int b = k / c.symbols;
     const int sidx = k - b * c.symbols;
-    s += __ldg(in + (int64_t)sidx * c.Qm + b);
+    const int64_t idx = (int64_t)sidx * c.Qm + b;
+    if (NRLDPC_INBOUNDS(idx, c.E, kBoundsLlr)) s += __ldg(in + idx);
   }
   return s;
 }
@@ -132,6 +133,8 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
     }
     __syncthreads();
     const int Zc = s_g.Zc, G = s_g.G, lq_len = s_g.lq_len;
+    // debug build: the graph's message planes fit the CTA's scratch (uniform over the CTA)
+    if (!NRLDPC_INBOUNDS(s_g.lr_off[s_g.R] - 1u, p.scratch_words, kBoundsScratch)) break;
     const int g = tid / Zc;
     const int zx = tid - g * Zc;
     const bool active = g < G;
@@ -176,7 +179,8 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
           } else {
             ab0 = ab1 = p.w_inline[bi][row];
           }
-          layer_dispatch<kDegenClip, true>(deg, p, s_g.edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, e0,
+          layer_dispatch<kDegenClip, true>(deg, p, s_g.edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
+                                           4u * (uint32_t)(G * lq_len), e0,
                                            (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
                                            (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, cur, fresh,
                                            scratch + s_g.lr_off[row] + tid);
@@ -191,8 +195,10 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
         const int4 gr = s_grp[gg];
         uint32_t r0 = 0u, r1 = 0u;
         const uint32_t w = i < lq_len ? s_lq[gg * lq_len + i] : 0u;
-        if (i < gr.x && (w & 0x8000u)) r0 = __ldg(p.crc_tab + gr.z + (gr.x - 1 - i));
-        if (i < gr.y && (w & 0x80000000u)) r1 = __ldg(p.crc_tab + gr.w + (gr.y - 1 - i));
+        if (i < gr.x && (w & 0x8000u) && NRLDPC_INBOUNDS(gr.x - 1 - i, kMaxB, kBoundsCrc))
+          r0 = __ldg(p.crc_tab + gr.z + (gr.x - 1 - i));
+        if (i < gr.y && (w & 0x80000000u) && NRLDPC_INBOUNDS(gr.y - 1 - i, kMaxB, kBoundsCrc))
+          r1 = __ldg(p.crc_tab + gr.w + (gr.y - 1 - i));
         r0 = __reduce_xor_sync(0xFFFFFFFFu, r0);
         r1 = __reduce_xor_sync(0xFFFFFFFFu, r1);
         if ((tid & 31) == 0) {
@@ -260,6 +266,8 @@ int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream) 
   count_launch();
   return (int)cudaGetLastError();
 }
+
+int bounds_read_mixed(uint32_t* out, bool reset) { return bounds_read_tu(out, reset); }
 
 int prepare_mixed(bool degen_clip) {
   const int smem = kThreadsTarget * kMaxCols * 4;

@@ -17,7 +17,9 @@
 //    more work items per CTA (slower than nrldpc_decode_batch, same results);
 //  * the first call on a device does the set-up for that device (symbol
 //    addresses, CRC table upload), so make that first call before any stream
-//    capture;
+//    capture; likewise the first algo-2 call after nrldpc_set_trained_weights
+//    changed a table copies the new table from host memory, so make that call
+//    before any capture too;
 //  * all calls share the arrays: calls that overlap on the GPU (different
 //    streams, or concurrent host threads) race on the scratch and must be
 //    serialised by the caller.  Nothing needs clearing between calls: the
@@ -159,9 +161,11 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
     const int k = cp.bgn == 1 ? 0 : 1;
     uint32_t* dst = nd->trained + (size_t)k * kNoAllocMaxTrainedIters * kMaxRows;
     if (nd->trained_gen[k] != gen) {
+      // Stream-ordered after earlier calls on this stream.  A copy from pageable
+      // host memory has read its source by the time it returns, so `ab` may go
+      // out of scope without a host synchronisation.
       if (cudaMemcpyAsync(dst, ab.data(), ab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                          reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess ||
-          cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+                          reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
         return NRLDPC_ERR_CUDA;
       nd->trained_gen[k] = gen;
     }

@@ -41,10 +41,11 @@ class MixedPlan:
     configs: per block (bgn, A, crctype, E, rv, Qm).  By default the LLRs of
     block i occupy llr_arena[llr_offsets[i] : llr_offsets[i] + E_i] and its
     hard bits bits_arena[bits_offsets[i] : + ceil(B_i/8)], packed back to back.
+    `lib` selects another build of the library (the bounds-checked debug one).
     """
 
-    def __init__(self, configs: Sequence[Sequence[int]], decoder_config, device=None):
-        self.lib = capi.load_library()
+    def __init__(self, configs: Sequence[Sequence[int]], decoder_config, device=None, lib=None):
+        self.lib = lib or capi.load_library()
         _declare(self.lib)
         self.configs = [tuple(int(v) for v in c[:6]) for c in configs]
         n = len(self.configs)

@@ -12,13 +12,20 @@ splits work across ranks and combines the per-rank timings:
 * ``max_over_ranks`` / ``sum_over_ranks`` — the step time of a multi-GPU job is
   the slowest rank's; processed units add up.  Both work with any
   ``torch.distributed`` backend (NCCL on GPUs, gloo on CPU) and with no process
-  group at all (single process).
+  group at all (single process);
+* ``torchrun_command`` / ``launch_ranks`` — start one process per GPU of this
+  node under ``torch.distributed.run`` (rendezvous on 127.0.0.1), so a script
+  asked for N GPUs outside a launcher can start its own ranks.
 """
 
 from __future__ import annotations
 
 import heapq
-from typing import List, Sequence, Tuple
+import os
+import socket
+import subprocess
+import sys
+from typing import List, Optional, Sequence, Tuple
 
 BG_NNZ = {1: 316, 2: 197}
 
@@ -79,3 +86,31 @@ def max_over_ranks(value: float, dist=None, device=None) -> float:
 def sum_over_ranks(value: float, dist=None, device=None) -> float:
     """Sum over all ranks (e.g. blocks or info bits processed)."""
     return _reduce(value, "SUM", dist, device)
+
+
+def free_port() -> int:
+    """An unused TCP port on 127.0.0.1 for the rendezvous."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def torchrun_command(nproc: int, script: str, argv: Sequence[str], port: int,
+                     timeout_s: Optional[int] = None) -> List[str]:
+    """Command line that runs `script argv` as `nproc` ranks on this node; with
+    `timeout_s` the whole launch is bounded (SIGTERM, then SIGKILL 60 s later)."""
+    if nproc < 1:
+        raise ValueError("nproc must be >= 1")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), script, *argv]
+    if timeout_s:
+        cmd = ["timeout", "-k", "60", str(int(timeout_s))] + cmd
+    return cmd
+
+
+def launch_ranks(nproc: int, script: str, argv: Sequence[str], timeout_s: Optional[int] = None,
+                 env: Optional[dict] = None) -> int:
+    """Run `script` as `nproc` ranks (stdout and stderr pass through); returns the
+    launcher's exit code."""
+    e = dict(os.environ if env is None else env)
+    return subprocess.call(torchrun_command(nproc, script, argv, free_port(), timeout_s), env=e)

@@ -198,7 +198,9 @@ int32_t nrldpc_decode_batch_host(const int16_t *h_llr, int64_t llr_stride,
  * tables are static device arrays of the library, held by every GPU that uses
  * this entry point until the process exits.  The first call on a device
  * resolves those arrays and uploads the CRC table, so make it before any
- * stream capture.  All calls share the arrays: calls that overlap on the GPU
+ * stream capture; the first algo-2 call after nrldpc_set_trained_weights
+ * changed a table uploads that table, so make it before any capture too.
+ * All calls share the arrays: calls that overlap on the GPU
  * race and must be serialised by the caller.  Returns -3 for algos 0 and 4,
  * -4 if an algo-2 table has more than 64 iterations or a configuration needs
  * more scratch per CTA than the array holds. */
@@ -469,6 +471,16 @@ int64_t nrldpc_kernel_launch_count(void);
 
 /* Library version string. */
 const char *nrldpc_version(void);
+
+/* No counterpart in the reference (its only checks are return codes).  Status
+ * of the device-side index checks of the debug build
+ * (libnrldpc_b200_debug.so, compiled with -DNRLDPC_BOUNDS_CHECK), which checks
+ * every gather and scatter index of the decode kernels and records the first
+ * violation instead of trapping: out[4] = {kind, index, limit, CTA} of that
+ * violation (kind 1 belief word, 2 edge entry, 3 message scratch, 4 LLR
+ * index, 5 CRC table entry; all zero when none), cleared when reset != 0.
+ * Returns 1 in the debug build, 0 in the release build (out all zero). */
+int32_t nrldpc_bounds_check_status(uint32_t *out, int32_t reset);
 
 #ifdef __cplusplus
 }

@@ -71,3 +71,28 @@ def demap(sym: np.ndarray, Qm: int, noise_power_db: float) -> np.ndarray:
         out.append(quantize(seg_llr(segs, re, A, nv)))
         out.append(quantize(seg_llr(segs, im, A, nv)))
     return np.stack(out, axis=-1)
+
+
+def bit_sign(b: np.ndarray) -> np.ndarray:
+    return np.where(b != 0, F(-1.0), F(1.0)).astype(F)
+
+
+def modulate(bits: np.ndarray, Qm: int) -> np.ndarray:
+    """bits uint8 [..., Qm] -> float32 [..., 2] NR constellation points, the
+    reference's float32 expressions in their order (c_lib/tx_rx_process.c:68-99)."""
+    A = F(1.0) / np.sqrt(F(NORM[Qm]), dtype=F)
+    s = [bit_sign(bits[..., j]) for j in range(Qm)]
+    if Qm == 1:
+        re = im = s[0] * A
+    elif Qm == 2:
+        re, im = s[0] * A, s[1] * A
+    elif Qm == 4:
+        re = (s[0] * (F(2.0) - s[2])) * A
+        im = (s[1] * (F(2.0) - s[3])) * A
+    elif Qm == 6:
+        re = (s[0] * (F(4.0) - s[2] * (F(2.0) - s[4]))) * A
+        im = (s[1] * (F(4.0) - s[3] * (F(2.0) - s[5]))) * A
+    else:
+        re = (s[0] * (F(8.0) - s[2] * (F(4.0) - s[4] * (F(2.0) - s[6])))) * A
+        im = (s[1] * (F(8.0) - s[3] * (F(4.0) - s[5] * (F(2.0) - s[7])))) * A
+    return np.stack([np.asarray(re, dtype=F), np.asarray(im, dtype=F)], axis=-1)

@@ -277,7 +277,29 @@ class RefLib:
         for acc in ("ref_fixed_lq", "ref_degree_lq", "ref_neural_lq"):
             getattr(L, acc).restype = ctypes.POINTER(ctypes.c_int16)
         L.ref_float_lq.restype = ctypes.POINTER(ctypes.c_float)
+        L.ref_modulate_symbols.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint16, ctypes.c_void_p]
+        L.ref_demap_symbols.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint16, ctypes.c_float,
+                                        ctypes.c_void_p, ctypes.c_void_p]
         self.libc = ctypes.CDLL(None)
+
+    def modulate_symbols(self, bits: np.ndarray, Qm: int) -> np.ndarray:
+        """The reference's modulate_symbol (c_lib/tx_rx_process.c:68) on each group
+        of Qm bits: uint8 [n, Qm] -> float32 [n, 2]."""
+        b = np.ascontiguousarray(bits, dtype=np.uint8).reshape(-1, Qm)
+        out = np.zeros((b.shape[0], 2), dtype=np.float32)
+        self.lib.ref_modulate_symbols(_p(b), b.shape[0], Qm, _p(out))
+        return out
+
+    def demap_symbols(self, sym: np.ndarray, Qm: int, noise_power_db: float, want_float: bool = False):
+        """The reference's demodulate_symbol + quantize_llr_to_int16
+        (c_lib/tx_rx_process.c:234, :27) on given noisy symbols float32 [n, 2],
+        with the noise variance computed as tx_rx_process does (:298)."""
+        s = np.ascontiguousarray(sym, dtype=np.float32).reshape(-1, 2)
+        q = np.zeros(s.shape[0] * Qm, dtype=np.int16)
+        f = np.zeros(s.shape[0] * Qm, dtype=np.float32) if want_float else None
+        self.lib.ref_demap_symbols(_p(s), s.shape[0], Qm, ctypes.c_float(noise_power_db), _p(q),
+                                   _p(f) if f is not None else None)
+        return (q, f) if want_float else q
 
     def srand(self, seed: int):
         self.libc.srand(ctypes.c_uint(seed))

@@ -19,7 +19,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
-sys.path.insert(0, "/root/reference")
+from oracle.refroot import REFERENCE_ROOT  # noqa: E402
+
+sys.path.insert(0, REFERENCE_ROOT)
 
 from py5gphy.ldpc import nr_ldpc_ratematch, nr_ldpc_raterecover  # noqa: E402
 

@@ -17,7 +17,10 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.refroot import REFERENCE_ROOT  # noqa: E402
+
+sys.path.insert(0, REFERENCE_ROOT)
 
 from py5gphy.crc import crc  # noqa: E402
 from py5gphy.ldpc import ldpc_info, nr_ldpc_ratematch  # noqa: E402

@@ -26,8 +26,9 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = "/root/reference"
 sys.path.insert(0, REPO)
+from oracle.refroot import REFERENCE_ROOT as REFERENCE  # noqa: E402
+
 sys.path.insert(0, REFERENCE)
 
 from deep_learning.deeplearning_ldpc_model import CTableNeuralLayeredMinSumDecoder  # noqa: E402

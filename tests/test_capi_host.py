@@ -37,6 +37,20 @@ def test_library_exports_every_declared_symbol(lib):
         assert getattr(lib, n) is not None
 
 
+def test_debug_library_exports_the_same_symbols_and_release_has_no_checks(lib):
+    from deeplearning_5g_ldpc_decoder_b200.build import DEBUG_LIB_PATH, build_library
+
+    path = DEBUG_LIB_PATH if os.path.exists(DEBUG_LIB_PATH) else build_library(debug=True)
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True)
+    exported = {line.split()[-1] for line in out.stdout.splitlines() if line.strip()}
+    for n in declared_functions():
+        assert n in exported, n
+    assert b"bounds-checked" in capi.load_library(path).nrldpc_version()
+    rec = (ctypes.c_uint32 * 4)(7, 7, 7, 7)
+    assert lib.nrldpc_bounds_check_status(rec, 1) == 0 and list(rec) == [0, 0, 0, 0]
+    assert b"bounds-checked" not in lib.nrldpc_version()
+
+
 def test_record_layouts_match_reference():
     assert ctypes.sizeof(capi.LdpcInConfig) == 14
     assert ctypes.sizeof(capi.DecoderConfig) == 14

@@ -86,3 +86,23 @@ def test_encode_channel_decode_chain_256qam(oracle, cuda):
         for i in range(0, 64, 8):
             es, eb, ei, _ = oracle.decode(host[i], in_config(*cfg), dec_cfg(row))
             assert st[i] == es and int(res.iterations[i]) == ei and np.array_equal(bits[i], eb), (esn0, i)
+
+
+@pytest.mark.parametrize("Qm", [1, 2, 4, 6, 8])
+def test_device_front_end_matches_reference_functions(cuda, reflib, Qm):
+    """The device mapper and demapper against the reference's own static
+    modulate_symbol / demodulate_symbol / quantize_llr_to_int16
+    (c_lib/tx_rx_process.c:27, :68, :234), called through the reference build's
+    channel shim.  At -300 dB of noise the noise term is far below half an ulp
+    of every constellation coordinate, so the device reports the clean points."""
+    rng = np.random.default_rng(40 + Qm)
+    n, E = 16, 1200 // Qm * Qm
+    rm = rng.integers(0, 256, size=(n, (E + 7) // 8), dtype=np.uint8)
+    bits = np.unpackbits(rm, axis=1)[:, :E].reshape(-1, Qm)
+    _, clean = channel_llrs(torch.from_numpy(rm).to(cuda), E, Qm, -300.0, seed=1, return_symbols=True)
+    want = reflib.modulate_symbols(bits, Qm)
+    assert np.array_equal(clean.cpu().numpy().reshape(-1, 2).view(np.uint32), want.view(np.uint32))
+    for noise_db in (-15.0, -2.0, 5.0):
+        llr, sym = channel_llrs(torch.from_numpy(rm).to(cuda), E, Qm, noise_db, seed=3, return_symbols=True)
+        want = reflib.demap_symbols(sym.cpu().numpy(), Qm, noise_db)
+        assert np.array_equal(llr.cpu().numpy().reshape(-1), want), noise_db

@@ -32,12 +32,13 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-def _decode(fn, llr, cfg, row, outs, stream):
+def _decode(fn, llr, cfg, row, outs, stream, harq=None):
     icfg = capi.make_in_config(*cfg)
     dcfg = capi.make_decoder_config(row)
     bits, status, iters, app = outs
     return fn(_ptr(llr), llr.shape[1], llr.shape[0], ctypes.byref(icfg), ctypes.byref(dcfg), _ptr(bits),
-              bits.shape[1], _ptr(status), _ptr(iters), _ptr(app), app.shape[1], ctypes.c_void_p(0), 0,
+              bits.shape[1], _ptr(status), _ptr(iters), _ptr(app), app.shape[1],
+              _ptr(harq) if harq is not None else ctypes.c_void_p(0), harq.shape[1] if harq is not None else 0,
               ctypes.c_void_p(stream))
 
 
@@ -74,8 +75,37 @@ def test_noalloc_matches_batched_entry_point_on_consecutive_calls(oracle, cuda, 
             for w, g in zip(want, got[call]):
                 assert torch.equal(w, g), (cfg, row, call)
         free.append(torch.cuda.mem_get_info(cuda)[0])
-        # After the per-device set-up of the first call, calls allocate nothing.
+        # After the per-device set-up of the very first call, calls allocate
+        # nothing, including the first call of a new configuration.
         assert abs(free[2] - free[1]) <= (2 << 20), free
+        if ci > 0:
+            assert abs(free[1] - free[0]) <= (2 << 20), (ci, free)
+
+
+def test_noalloc_combines_into_soft_buffers_like_batched_entry_point(oracle, cuda, lib):
+    """HARQ: an rv 2 retransmission combined into the soft buffers an rv 0
+    transmission left; every call starts from copies of the same buffers."""
+    stream = torch.cuda.current_stream(cuda).cuda_stream
+    row = [1, 10, 22936, 0, 1280, 32767, -32767]
+    first, retx = (2, 488, 1, 1920, 0, 2, 0), (2, 488, 1, 1920, 2, 2, 1)
+    n = 96
+    p = capi.gen_ldpc_parameters(capi.make_in_config(*first))
+    llr0 = torch.from_numpy(_inputs(oracle, first, n, seed=11)).to(cuda)
+    llr2, _ = make_llrs(oracle, in_config(*retx[:6], 0), 48, noise_db=0.5, seed=12)
+    llr2 = torch.from_numpy(np.ascontiguousarray(np.tile(llr2, (2, 1)))).to(cuda)
+    stored = torch.zeros((n, p.N + 2 * p.Zc), dtype=torch.int16, device=cuda)
+    assert _decode(lib.nrldpc_decode_batch, llr0, first, row, _outputs(n, first, cuda), stream, stored) == 0
+    want, want_h = _outputs(n, retx, cuda), stored.clone()
+    assert _decode(lib.nrldpc_decode_batch, llr2, retx, row, want, stream, want_h) == 0
+    torch.cuda.synchronize(cuda)
+    assert not torch.equal(want_h, stored)
+    for call in range(2):
+        got, got_h = _outputs(n, retx, cuda), stored.clone()
+        assert _decode(lib.nrldpc_decode_batch_noalloc, llr2, retx, row, got, stream, got_h) == 0
+        torch.cuda.synchronize(cuda)
+        for w, g in zip(want, got):
+            assert torch.equal(w, g), call
+        assert torch.equal(want_h, got_h), call
 
 
 def test_noalloc_rejects_float_algorithms(cuda, lib):
