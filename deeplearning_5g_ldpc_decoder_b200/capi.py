@@ -80,7 +80,9 @@ class ServeConfig(ctypes.Structure):
 
     _fields_ = [("max_batch_tbs", ctypes.c_int32), ("max_batch_cbs", ctypes.c_int32),
                 ("llr_budget_bytes", ctypes.c_int64), ("pipeline_depth", ctypes.c_int32), ("pad", ctypes.c_int32),
-                ("timeout_s", ctypes.c_double)]
+                ("timeout_s", ctypes.c_double), ("max_wait_s", ctypes.c_double),
+                ("h_cb_first", ctypes.c_void_p), ("d_cb_bits", ctypes.c_void_p), ("d_cb_status", ctypes.c_void_p),
+                ("d_cb_iterations", ctypes.c_void_p)]
 
 
 class ServeStats(ctypes.Structure):
@@ -88,10 +90,11 @@ class ServeStats(ctypes.Structure):
 
     _fields_ = [("admitted", ctypes.c_int64), ("dropped", ctypes.c_int64), ("completed", ctypes.c_int64),
                 ("failed", ctypes.c_int64), ("batches", ctypes.c_int64), ("wall_s", ctypes.c_double),
-                ("mean_batch_tbs", ctypes.c_double)]
+                ("mean_batch_tbs", ctypes.c_double), ("expired", ctypes.c_int64)]
 
 
 NRLDPC_TB_DROPPED = -5
+NRLDPC_TB_EXPIRED = -6
 NRLDPC_TB_HARQ_COMBINE = 1
 NRLDPC_TB_HARQ_STORE = 2
 

@@ -451,6 +451,31 @@ int engine_decode(TbEngine* e, int lane, const nrldpc_tb_t* d_tbs, int n, const 
   return cudaGetLastError() == cudaSuccess ? NRLDPC_OK : NRLDPC_ERR_CUDA;
 }
 
+// Serving's optional per-code-block record: the batch's code blocks sit in
+// transport-block order in the lane (the segmentation kernel's scan), so
+// member j's start is the sum of the C of the members before it.
+int record_code_blocks(TbEngine* e, int lane, const nrldpc_serve_cfg_t* cfg, const std::vector<int>& members,
+                       const std::vector<int>& ncb, cudaStream_t s) {
+  const TbLane* l = e->lanes[lane];
+  int first = 0;
+  for (int i : members) {
+    const int C = ncb[i];
+    const int64_t dst = cfg->h_cb_first[i];
+    if ((cfg->d_cb_status &&
+         cudaMemcpyAsync(cfg->d_cb_status + dst, l->d_cb_status + first, (size_t)C * sizeof(int32_t),
+                         cudaMemcpyDeviceToDevice, s) != cudaSuccess) ||
+        (cfg->d_cb_iterations &&
+         cudaMemcpyAsync(cfg->d_cb_iterations + dst, l->d_cb_iters + first, (size_t)C * sizeof(int32_t),
+                         cudaMemcpyDeviceToDevice, s) != cudaSuccess) ||
+        (cfg->d_cb_bits &&
+         cudaMemcpyAsync(cfg->d_cb_bits + dst * kCbBitsStride, l->d_cb_bits + (int64_t)first * kCbBitsStride,
+                         (size_t)C * kCbBitsStride, cudaMemcpyDeviceToDevice, s) != cudaSuccess))
+      return NRLDPC_ERR_CUDA;
+    first += C;
+  }
+  return NRLDPC_OK;
+}
+
 double now_s() {
   using clk = std::chrono::steady_clock;
   return std::chrono::duration<double>(clk::now().time_since_epoch()).count();
@@ -711,6 +736,17 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
       progress = true;
     }
     if (rc != NRLDPC_OK) break;
+    // admitted blocks past their wait bound leave the queue (it is in arrival order)
+    while (cfg->max_wait_s > 0.0 && !ready.empty() && t - arrival_s[ready.front()] > cfg->max_wait_s) {
+      const int i = ready.front();
+      ready.pop_front();
+      h_status[i] = NRLDPC_TB_EXPIRED;
+      h_latency_s[i] = NAN;
+      budget_used -= 2 * (int64_t)tbs[i].G;
+      st.expired++;
+      done++;
+      progress = true;
+    }
     // arrivals: admit into the LLR budget or drop
     while (next < n && arrival_s[next] <= t) {
       const int64_t bytes = 2 * (int64_t)tbs[next].G;
@@ -752,6 +788,7 @@ int32_t nrldpc_serve_run(void* engine, const nrldpc_serve_cfg_t* cfg, const nrld
           engine_decode(e, k, sl.d_tbs, m, d_llr, d_out, sl.d_status, nullptr, nullptr, ss) != NRLDPC_OK ||
           cudaMemcpyAsync(sl.h_status, sl.d_status, (size_t)m * sizeof(int32_t), cudaMemcpyDeviceToHost, ss) !=
               cudaSuccess ||
+          (cfg->h_cb_first && record_code_blocks(e, k, cfg, sl.members, ncb, ss) != NRLDPC_OK) ||
           cudaEventRecord(sl.ev, ss) != cudaSuccess) {
         rc = NRLDPC_ERR_CUDA;
         break;

@@ -172,14 +172,22 @@ class TbEngine:
 
 @dataclass
 class ServeResult:
-    status: np.ndarray        # int32 per block: 0 pass, 1 fail, -5 dropped, -2 bad configuration
-    latency_s: np.ndarray     # verdict - arrival (NaN when dropped)
+    status: np.ndarray        # int32 per block: 0 pass, 1 fail, -5 dropped, -6 expired, -2 bad configuration
+    latency_s: np.ndarray     # verdict - arrival (NaN when dropped or expired)
     stats: dict
+    cb_first: Optional[np.ndarray] = None   # with record=True: block i's code blocks start here in
+    cb_status: Optional[np.ndarray] = None  # the per-code-block status, iterations and hard bits
+    cb_iterations: Optional[np.ndarray] = None
+    cb_bits: Optional[np.ndarray] = None    # [code blocks][1056] bytes
 
 
 def serve(engine: TbEngine, tbs: np.ndarray, arrival_s: np.ndarray, llr, out, *, max_batch_tbs: int = 4096,
           max_batch_cbs: Optional[int] = None, llr_budget_bytes: int = 8 << 30, pipeline_depth: int = 2,
-          timeout_s: float = 120.0, stream=None) -> ServeResult:
+          timeout_s: float = 120.0, max_wait_s: float = 0.0, record: bool = False, stream=None) -> ServeResult:
+    """Serve an arrival trace through the native loop (nrldpc_serve_run).
+    max_wait_s > 0 drops admitted blocks that wait longer for a batch
+    (NRLDPC_TB_EXPIRED); record=True also returns every decoded code block's
+    status, iterations and hard bits (a device copy per block: for checks)."""
     import torch
 
     n = len(tbs)
@@ -188,7 +196,20 @@ def serve(engine: TbEngine, tbs: np.ndarray, arrival_s: np.ndarray, llr, out, *,
     status = np.zeros(n, dtype=np.int32)
     lat = np.zeros(n, dtype=np.float64)
     cfg = capi.ServeConfig(int(max_batch_tbs), int(max_batch_cbs or engine.max_cbs), int(llr_budget_bytes),
-                           int(pipeline_depth), 0, float(timeout_s))
+                           int(pipeline_depth), 0, float(timeout_s), float(max_wait_s))
+    rec = None
+    if record:
+        counts = np.array([segment(int(t["A"]), int(t["G"]), int(t["Qm"]), int(t["bgn"]), int(t["rv"]),
+                                   int(t["tbs_lbrm"])).C for t in tbs], dtype=np.int64)
+        first = np.ascontiguousarray(np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int64))
+        total = max(int(counts.sum()), 1)
+        rec = (first, torch.full((total,), -9, dtype=torch.int32, device=llr.device),
+               torch.full((total,), -9, dtype=torch.int32, device=llr.device),
+               torch.zeros((total, 1056), dtype=torch.uint8, device=llr.device))
+        cfg.h_cb_first = first.ctypes.data
+        cfg.d_cb_status = rec[1].data_ptr()
+        cfg.d_cb_iterations = rec[2].data_ptr()
+        cfg.d_cb_bits = rec[3].data_ptr()
     st = capi.ServeStats()
     s = stream if stream is not None else torch.cuda.current_stream(llr.device)
     rc = engine.lib.nrldpc_serve_run(engine.handle, ctypes.byref(cfg), tbs.ctypes.data_as(ctypes.c_void_p),
@@ -199,7 +220,10 @@ def serve(engine: TbEngine, tbs: np.ndarray, arrival_s: np.ndarray, llr, out, *,
     if rc != 0:
         raise RuntimeError(f"nrldpc_serve_run failed: {rc}")
     stats = {k: getattr(st, k) for k, _ in capi.ServeStats._fields_}
-    return ServeResult(status, lat, stats)
+    if rec is None:
+        return ServeResult(status, lat, stats)
+    s.synchronize()
+    return ServeResult(status, lat, stats, rec[0], rec[1].cpu().numpy(), rec[2].cpu().numpy(), rec[3].cpu().numpy())
 
 
 def tb_crc(payload: np.ndarray, A: int) -> np.ndarray:

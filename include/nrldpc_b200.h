@@ -290,6 +290,7 @@ int32_t nrldpc_mixed_plan_destroy(void *plan);
  * py5gphy/ldpc/ldpc_info.py:59-109 and py5gphy/ldpc/nr_ldpc_ratematch.py:22-45) */
 
 #define NRLDPC_TB_DROPPED (-5)   /* serving: not admitted (HBM budget exhausted) */
+#define NRLDPC_TB_EXPIRED (-6)   /* serving: admitted, but waited longer than max_wait_s for a batch */
 
 /* One transport block: A payload bits (multiple of 8), coded into G bits
  * (multiple of Qm, one layer) on base graph bgn.  Its G int16 LLRs start at
@@ -376,20 +377,34 @@ typedef struct {
     int32_t pipeline_depth;     /* batches in flight, 1..16 (one engine lane each: ~90 MB of scratch) */
     int32_t pad;
     double timeout_s;           /* the run fails with NRLDPC_ERR_CUDA after this long */
+    double max_wait_s;          /* > 0: an admitted block that has waited longer than this for a
+                                   batch is dropped (NRLDPC_TB_EXPIRED), which bounds the queueing
+                                   part of the latency past saturation; 0: no bound */
+    /* Optional record of every decoded code block (all NULL: none).  Block i's
+     * C code blocks go to indices h_cb_first[i] .. + C of the device arrays:
+     * hard bits [..][1056] bytes, status and iterations.  Costs a device copy
+     * per transport block: a checking aid, not for production. */
+    const int64_t *h_cb_first;
+    uint8_t *d_cb_bits;
+    int32_t *d_cb_status;
+    int32_t *d_cb_iterations;
 } nrldpc_serve_cfg_t;
 
 typedef struct {
     int64_t admitted, dropped, completed, failed, batches;
     double wall_s;              /* first arrival to last verdict */
     double mean_batch_tbs;
+    int64_t expired;            /* admitted blocks dropped after max_wait_s */
 } nrldpc_serve_stats_t;
 
 /* Run the arrival trace tbs[i] / arrival_s[i] (host arrays, arrival times in
  * seconds from the start of the call, ascending) through the engine with
  * continuous batching: a block is admitted on arrival if its LLR bytes fit the
  * budget (else dropped: status NRLDPC_TB_DROPPED), admitted blocks form a new
- * batch whenever fewer than pipeline_depth batches are in flight, and each
- * block's verdict time is taken when its batch's completion event is observed.
+ * batch whenever fewer than pipeline_depth batches are in flight (an admitted
+ * block that waits longer than max_wait_s, when set, is dropped:
+ * NRLDPC_TB_EXPIRED), and each block's verdict time is taken when its batch's
+ * completion event is observed.
  * Writes h_status [n] and h_latency_s [n] (verdict - arrival; NaN if dropped).
  * All waits are host polls bounded by timeout_s; no device-side waits. */
 int32_t nrldpc_serve_run(void *engine, const nrldpc_serve_cfg_t *cfg, const nrldpc_tb_t *tbs,

@@ -80,3 +80,41 @@ def test_mixed_lane_refill_bit_exact(oracle, cuda):
         assert np.array_equal(b[plan.bits_offsets[i]: plan.bits_offsets[i] + plan.nbytes[i]], eb), (i, c)
     assert len(set(it.tolist())) >= 5      # blocks finish at many different iterations
     plan.close()
+
+
+def test_config3_full_batch_every_block_matches_oracle(cuda):
+    """The mixed-size workload at its full size: 32768 code blocks, lifting
+    sizes uniform over all 51, BG1 60 %, rate U[0.2, 0.92], Qm {2, 4, 6, 8},
+    algo 1, 10 iterations, decoded in one persistent launch from a CUDA graph.
+    Every block's status, iteration count and hard bits equal the oracle
+    decoding that block alone (on all host cores)."""
+    from deeplearning_5g_ldpc_decoder_b200 import channel_llrs, ldpc_encode
+    from tests.oracle_pool import oracle_decode_blocks
+
+    n = 32768
+    cfgs = random_mixed_configs(n, seed=2024, rvs=(0,))
+    gen = torch.Generator(device=cuda).manual_seed(7)
+    llrs = []
+    for i, (bgn, A, crc, E, rv, Qm) in enumerate(cfgs):
+        pay = torch.randint(0, 256, (1, A // 8), dtype=torch.uint8, device=cuda, generator=gen)
+        eta = (A + 24) / E * Qm
+        snr = 10.0 * np.log10(2.0 ** eta - 1.0) + 3.0 + 0.5 * (i % 5)
+        llrs.append(channel_llrs(ldpc_encode(pay, (bgn, A, crc, E, rv, Qm, 0)), E, Qm, -snr, seed=i)[0])
+    row = [1, 10, 22936, 0, 1280, 32767, -32767]
+    plan = MixedPlan(cfgs, row, device=cuda)
+    arena = torch.cat(llrs)
+    stream = torch.cuda.Stream(cuda)
+    with torch.cuda.stream(stream):
+        plan.decode(arena, use_graph=True)
+        bits, status, iters = plan.decode(arena, use_graph=True)
+    stream.synchronize()
+    st, it, b = status.cpu().numpy(), iters.cpu().numpy(), bits.cpu().numpy()
+    est, eit, ebits = oracle_decode_blocks(arena.cpu().numpy(), cfgs, plan.llr_offsets, row)
+    bad_status = np.nonzero((st != est) | (it != eit))[0]
+    bad_bits = [i for i in range(n)
+                if eit[i] > 0 and not np.array_equal(b[plan.bits_offsets[i]: plan.bits_offsets[i] + plan.nbytes[i]],
+                                                     ebits[i])]
+    assert len(bad_status) == 0 and len(bad_bits) == 0, (bad_status[:10], bad_bits[:10])
+    conv = int((est == 0).sum())
+    assert 0.5 * n < conv < n and len(set(eit.tolist())) >= 5
+    plan.close()

@@ -274,3 +274,60 @@ def test_harq_retransmission_with_limited_buffer(cuda, oracle):
                 assert np.array_equal(out.cpu().numpy()[o:o + int(t["A"]) // 8], pays[i])
         passed.append(int((st == 0).sum()))
     assert passed[1] > passed[0]
+
+
+def test_serving_depth8_every_code_block_decodes_as_alone(cuda, oracle):
+    """Poisson arrivals through the serving loop with eight batches in flight:
+    batches overlap on the device and their composition depends on timing.
+    Every code block's status, iteration count and hard bits inside the serve
+    run equal the oracle decoding that code block alone, and every transport
+    block's verdict equals the oracle's."""
+    from deeplearning_5g_ldpc_decoder_b200.tb import TbEngine, serve
+
+    rng = np.random.default_rng(61)
+    specs = []
+    for k in range(72):
+        A0 = float(np.exp(rng.uniform(np.log(200), np.log(120000))))
+        Qm = int(rng.choice([2, 4, 6, 8]))
+        R = float(rng.uniform(0.3, 0.85))
+        snr = {2: 3.0, 4: 9.0, 6: 14.0, 8: 20.0}[Qm] + 10 * (R - 0.5) + rng.uniform(-2.0, 5.0)
+        specs.append((A0, R, Qm, snr))
+    tbs, arena, out_bytes, pays = _traffic(rng, specs, cuda)
+    eng = TbEngine(max_tbs=64, max_cbs=2048, decoder_row=ROW)
+    out = torch.zeros(out_bytes + 8, dtype=torch.uint8, device=cuda)
+    arrivals = np.cumsum(rng.exponential(1.0 / 20000.0, len(tbs)))     # Poisson, 20k blocks/s
+    res = serve(eng, tbs, arrivals, arena, out, max_batch_tbs=8, pipeline_depth=8, timeout_s=60.0, record=True)
+    assert res.stats["completed"] == len(tbs) and res.stats["dropped"] == 0 and res.stats["expired"] == 0
+    assert res.stats["batches"] >= 9          # more batches than slots: slots were reused while others ran
+    arena_h = arena.cpu().numpy()
+    n_cb = 0
+    for i in range(len(tbs)):
+        exp, tb_st, info = _expected(oracle, tbs, arena_h, i)
+        f = int(res.cb_first[i])
+        for r, (st, bits, it) in enumerate(exp):
+            assert (res.cb_status[f + r], res.cb_iterations[f + r]) == (st, it), (i, r)
+            if it > 0:
+                assert np.array_equal(res.cb_bits[f + r][: len(bits)], bits), (i, r)
+        assert res.status[i] == tb_st, i
+        n_cb += len(exp)
+    assert n_cb > 2 * len(tbs)
+    assert 0 < (res.status == 0).sum() < len(tbs)
+
+
+def test_serving_wait_bound_expires_queued_blocks(cuda):
+    """With one batch in flight, one block per batch and everything arriving at
+    once, blocks still queued after max_wait_s are dropped as expired (their
+    budget freed, latency NaN); the ones served are decoded normally."""
+    from deeplearning_5g_ldpc_decoder_b200.tb import TbEngine, serve
+
+    rng = np.random.default_rng(23)
+    tbs, arena, out_bytes, _ = _traffic(rng, [(60000, 0.5, 4, 20.0)] * 30, cuda)
+    eng = TbEngine(max_tbs=4, max_cbs=64, decoder_row=ROW)
+    out = torch.zeros(out_bytes + 8, dtype=torch.uint8, device=cuda)
+    res = serve(eng, tbs, np.zeros(len(tbs)), arena, out, max_batch_tbs=1, pipeline_depth=1, timeout_s=30.0,
+                max_wait_s=1e-4)
+    expired = res.status == -6
+    assert expired.sum() == res.stats["expired"] > 0
+    assert np.all(res.status[~expired] == 0) and (~expired).sum() >= 1
+    assert np.all(np.isnan(res.latency_s[expired])) and np.all(np.isfinite(res.latency_s[~expired]))
+    assert res.stats["completed"] + res.stats["expired"] == len(tbs)
