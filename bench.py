@@ -14,9 +14,23 @@ step (415 MB) exceed the 126 MB L2, so no flush is needed between steps.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 Prints one JSON line (rank 0).  N>1 runs one process per GPU under
-torch.distributed.run; every rank decodes its own 8192 blocks (weak scaling,
-no collective on the data path; NCCL only for the barrier and the max-time
-reduction).
+torch.distributed.run (started here when no launcher did); every rank decodes
+its own 8192 blocks (weak scaling, no collective on the data path; NCCL only
+for the barrier and the max-time reduction).
+
+Besides the timed step, the default single-GPU run adds, as extra keys of the
+same line:
+  * early_exit / config2_variants: device-encoded blocks through the 256QAM
+    channel near the 1e-2 point (E=25344 algo 1, E=9600 algo 1, E=25344 BP);
+  * parity: every block of the timed step and of those legs decoded again by
+    the reference C decoder (oracle/_ref, one process per host core) and
+    compared block by block; the same run gives cpu_baseline;
+  * per_call: drop-in latency on the reference CUDA test's 8 cases;
+  * mixed, serve, train: the mixed-size batch (every block checked against
+    the reference), the serving loop and a training step, each with its own
+    clock record (--no-legs skips them).
+--impl reference times the reference C decoder alone on the GPU arm's own
+blocks.
 """
 
 from __future__ import annotations
@@ -715,7 +729,7 @@ def run_mixed(args):
     import torch
 
     from deeplearning_5g_ldpc_decoder_b200 import capi, channel_llrs, ldpc_decode, ldpc_encode
-    from deeplearning_5g_ldpc_decoder_b200.mixed import MixedPlan, random_mixed_configs
+    from deeplearning_5g_ldpc_decoder_b200.mixed import AUTOTUNE_NAMES, MixedPlan, random_mixed_configs
 
     n = args.n_cw if args.n_cw != N_CW else 32768
     row = [1, 10, 22936, 0, 1280, 32767, -32767]
@@ -794,8 +808,7 @@ def run_mixed(args):
                                          "path": "nrldpc_decode_batch once per block (C ABI), same inputs"},
             "speedup_vs_plain": round(ms_plain / ms_mixed, 2),
             "autotune": {"chosen": best, "candidates_ms": [round(x, 4) for x in cand_ms],
-                         "candidates": ["2 CTA/SM largest-first", "1 CTA/SM largest-first",
-                                        "2 CTA/SM interleaved", "1 CTA/SM interleaved"]},
+                         "candidates": AUTOTUNE_NAMES},
             "iterations_executed_mean": float(iters.float().mean().item()), "bler": float(1.0 - ok.mean()),
             "parity": parity, "gpu_launches": int(launches)}
 

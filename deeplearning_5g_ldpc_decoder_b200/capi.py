@@ -137,6 +137,7 @@ EXPORTED_SYMBOLS = (
     "nrldpc_mixed_plan_create",
     "nrldpc_mixed_plan_execute",
     "nrldpc_mixed_plan_autotune",
+    "nrldpc_mixed_plan_select",
     "nrldpc_mixed_plan_destroy",
     "nrldpc_tb_segment",
     "nrldpc_tb_select_bg",

@@ -251,6 +251,8 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
     int e = trained_device_table(st, cp.bgn, &p.weights, &p.weights_T);
     if (e) return e;
   }
+  p.rr_scatter = fixed && cp.E <= cp.Nv;
+  p.qm_magic = qm_magic(cp.Qm);
   p.f_alpha = (float)dc.alpha / 32768.0f;
   p.f_beta = (float)dc.beta / 128.0f;
   p.f_max = (float)dc.max_llr / 128.0f;
@@ -266,7 +268,7 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
     if (algo == 0) {
       planes = deg;
     } else if (fixed) {
-      planes = deg > 16 ? 5 : 4;
+      planes = fixed_row_planes(deg);
     } else {
       planes = 4;
     }
@@ -349,6 +351,7 @@ int32_t decode_batch_locked(const int16_t* d_llr, int64_t llr_stride, int32_t nu
   }
   p.llr = d_llr;
   p.llr_stride = llr_stride;
+  p.rr_vec = (reinterpret_cast<uintptr_t>(d_llr) % 16 == 0) && (llr_stride % 8 == 0);
   p.bits = d_bits;
   p.bits_stride = bits_stride;
   p.status = d_status;

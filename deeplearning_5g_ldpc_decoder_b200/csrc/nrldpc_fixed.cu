@@ -185,8 +185,9 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
     if (active) {
       cw[0] = s_base + 2 * g < p.num_cw ? s_base + 2 * g : -1;
       cw[1] = s_base + 2 * g + 1 < p.num_cw ? s_base + 2 * g + 1 : -1;
-      recover_halves(p, lq, zx, cw[0], cw[1], true, true);
+      if (!p.rr_scatter) recover_halves(p, lq, zx, cw[0], cw[1], true, true);
     }
+    if (p.rr_scatter) recover_scatter(p, lq, zx, active, cw[0], cw[1], true, true);
     uint32_t itv = 0u;   // iterations of half 0 in bits 0-15, half 1 in bits 16-31
     if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
     uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
@@ -249,8 +250,10 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
           itv &= h ? 0x0000FFFFu : 0xFFFF0000u;
           if (cw[h] >= 0) fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
         }
-        recover_halves(p, lq, zx, cw[0], cw[1], fin[0], fin[1]);
+        if (!p.rr_scatter) recover_halves(p, lq, zx, cw[0], cw[1], fin[0], fin[1]);
       }
+      // `any` is uniform here, so every thread of the CTA reaches the barriers inside
+      if (p.rr_scatter) recover_scatter(p, lq, zx, active, cw[0], cw[1], fin[0], fin[1]);
       idle = __syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0));
     }
     // Every take of this CTA is done (the last barrier above).  The CTA that
@@ -270,7 +273,8 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
       const bool v1 = active && cw1 < p.num_cw;
 
       // ---- rate recovery into LQ (and the soft buffers) ----
-      if (active) {
+      if (p.rr_scatter) recover_scatter(p, lq, zx, active, v0 ? cw0 : -1, v1 ? cw1 : -1, true, true);
+      if (active && !p.rr_scatter) {
         const int16_t* in0 = p.llr + (int64_t)(v0 ? cw0 : 0) * p.llr_stride;
         const int16_t* in1 = p.llr + (int64_t)(v1 ? cw1 : 0) * p.llr_stride;
         int16_t* h0 = (p.harq && v0) ? p.harq + (int64_t)cw0 * p.harq_stride : nullptr;

@@ -55,6 +55,24 @@ uint32_t crc_remainder(const uint8_t* data, int len, int crctype);
 // message whose only set bit sits d positions before its end.
 void crc_position_table(int crctype, uint32_t* out /* kMaxB */);
 
+// Scratch planes (kThreadsTarget words each) of one lifted check row of degree
+// d in the fixed-point kernels: the two minima, the flip bits and the min2
+// bits, plus a fifth word for degree-19 rows (layout in nrldpc_fixed_row.cuh).
+inline int fixed_row_planes(int d) { return d > 16 ? 5 : 4; }
+// Scratch words per CTA of the mixed-size kernel: the larger of the two base
+// graphs' layouts (all rows' planes x kThreadsTarget).
+uint32_t mixed_scratch_words_per_cta();
+
+// ceil(2^32 / Qm), the constant that turns e / Qm into one high multiply in the
+// kernels' scatter-form rate recovery (div_qm); 0 for Qm = 1, whose quotient is
+// e itself (its constant, 2^32, does not fit 32 bits).
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline uint32_t qm_magic(int qm) {
+  return qm <= 1 ? 0u : (uint32_t)((0x100000000ull + (uint64_t)qm - 1) / (uint64_t)qm);
+}
+
 // Alpha/beta per (iteration, row): alpha in the low 16 bits, beta in the high.
 inline uint32_t pack_ab(int16_t alpha, int16_t beta) {
   return (uint32_t)(uint16_t)alpha | ((uint32_t)(uint16_t)beta << 16);
@@ -71,6 +89,9 @@ struct DecodeParams {
   int32_t harq_on;
   int32_t fill, max_llr, min_llr;
   int32_t weights_T;   // 0: use w_inline[row]; >0: weights[min(it,T-1)*R + row]
+  int32_t rr_scatter;  // rate recovery in scatter form (E <= Nv: no LLR repeats), fixed-point kernel
+  int32_t rr_vec;      // LLR rows 16-byte aligned: 8 LLRs per load in the scatter form
+  uint32_t qm_magic;   // ceil(2^32 / Qm): e / Qm as __umulhi(e, qm_magic) for e < 2^16
   float f_alpha, f_beta, f_max, f_min;
   const uint32_t* weights;
   const uint32_t* crc_tab;
@@ -192,9 +213,14 @@ int launch_encode(const EncodeParams& p, void* stream);
 int launch_train_forward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream);
 int launch_train_backward(const TrainParams& p, bool f64, int grid, int block, int smem, void* stream);
 int occupancy_train(bool backward, bool f64, bool bg2, int block, int smem, bool alias = false);
-int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream);
-int prepare_mixed(bool degen_clip);
-int occupancy_mixed(bool degen_clip);
+// Mixed-size kernel classes: 0 = 384 threads per CTA (all of them active at
+// most), 1 = 256 threads with at most 240 active, three CTAs per SM.  A graph
+// of a class holds G = floor(capacity / Zc) lane pairs per CTA.
+constexpr int kMixedClasses = 2;
+int mixed_class_capacity(int cls);
+int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream, int cls = 0);
+int prepare_mixed(bool degen_clip, int cls = 0);
+int occupancy_mixed(bool degen_clip, int cls = 0);
 int launch_channel(const uint8_t* rm, int64_t rm_stride, int32_t num_cw, int32_t E, int32_t Qm, float nv,
                    float sigma, float A, uint64_t seed, int16_t* llr, int64_t llr_stride, float* symbols,
                    void* stream);

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "nrldpc_decode_common.cuh"
 #include "nrldpc_fixed_row.cuh"
 #include "nrldpc_internal.h"
 
@@ -85,30 +86,89 @@ __device__ __forceinline__ int take_block(const MixedParams& p, int key) {
   return i < p.key_count[key] ? p.cb_list[p.key_base[key] + i] : -1;
 }
 
-// Rate recovery of block cw into half h of the group's LQ words (the other
-// half is kept), with its HARQ soft buffer.
-__device__ __forceinline__ void recover_half(const MixedParams& p, const MixedGraph& g, int cw, int h, uint32_t* lq,
-                                             int zx) {
-  const MixedCw c = p.cws[cw];
-  const int16_t* in = p.llr + c.llr_off;
-  int16_t* hq = (c.harq_mode && p.harq) ? p.harq + c.harq_off : nullptr;
-  const int shift = 16 * h;
-  const uint32_t keep = h ? 0x0000FFFFu : 0xFFFF0000u;
-  for (int i = zx; i < g.lq_len; i += g.Zc) {
-    const int32_t init = (hq && (c.harq_mode & 1)) ? hq[i] : 0;
-    const int32_t a = mixed_recover(g, c, in, i, p.fill, init);
-    if (hq && (c.harq_mode & 2)) hq[i] = (int16_t)a;
-    lq[i] = (lq[i] & keep) | (((uint32_t)a & 0xFFFFu) << shift);
+// Rate recovery of the refreshed halves (r_h) of a group's LQ words: half h gets
+// block cw_h, zeros when cw_h < 0; the other half keeps its bits.  Blocks with
+// E <= Nv (no LLR repeats) use the scatter form: (A) base values (filler, the
+// stored soft buffer when combining, else 0), (B) each LLR, read with 16-byte
+// loads where the row is aligned, added to its own position (int16 wrap-around),
+// (C) the soft buffer stored.  Blocks with repetitions take the gather form in
+// (A).  Called by every thread of the CTA (CTA barriers inside).
+__device__ __noinline__ void recover_halves_mixed(const MixedParams& p, const MixedGraph& g, uint32_t* lq, int zx, bool active,
+                                     const int* cw, bool r0, bool r1) {
+  const bool rr[2] = {r0, r1};
+  bool scat[2] = {false, false};
+  if (active) {
+    const uint32_t keep = (r0 ? 0u : 0x0000FFFFu) | (r1 ? 0u : 0xFFFF0000u);
+    if (r0 || r1)
+      for (int i = zx; i < g.lq_len; i += g.Zc) lq[i] &= keep;
+    for (int h = 0; h < 2; ++h) {
+      if (!rr[h] || cw[h] < 0) continue;
+      const MixedCw c = p.cws[cw[h]];
+      scat[h] = c.E <= c.Nv;
+      int16_t* hq = (c.harq_mode && p.harq) ? p.harq + c.harq_off : nullptr;
+      const int shift = 16 * h;
+      if (scat[h]) {
+        for (int i = zx; i < g.lq_len; i += g.Zc) {
+          const int32_t a = (i >= c.B && i < g.K) ? p.fill : ((hq && (c.harq_mode & 1)) ? hq[i] : 0);
+          lq[i] |= ((uint32_t)a & 0xFFFFu) << shift;
+        }
+      } else {
+        const int16_t* in = p.llr + c.llr_off;
+        for (int i = zx; i < g.lq_len; i += g.Zc) {
+          const int32_t init = (hq && (c.harq_mode & 1)) ? hq[i] : 0;
+          const int32_t a = mixed_recover(g, c, in, i, p.fill, init);
+          if (hq && (c.harq_mode & 2)) hq[i] = (int16_t)a;
+          lq[i] |= ((uint32_t)a & 0xFFFFu) << shift;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  int16_t* lq16 = reinterpret_cast<int16_t*>(lq);
+  const int twoZ = 2 * g.Zc;
+  for (int h = 0; h < 2; ++h) {
+    if (!scat[h]) continue;
+    const MixedCw c = p.cws[cw[h]];
+    const int16_t* in = p.llr + c.llr_off;
+    const uint32_t magic = qm_magic(c.Qm);
+    const uint32_t E = (uint32_t)c.E;
+    auto add = [&](uint32_t e, int16_t x) {
+      const uint32_t s = div_qm(e, (uint32_t)c.Qm, magic);
+      int cc = c.c0 + (int)((e - s * (uint32_t)c.Qm) * (uint32_t)c.symbols + s);
+      cc -= cc >= c.Nv ? c.Nv : 0;
+      const int pos = (cc < c.B - twoZ ? cc : cc + c.F) + twoZ;
+      if (NRLDPC_INBOUNDS(pos, g.lq_len, kBoundsLq)) lq16[2 * pos + h] = (int16_t)(lq16[2 * pos + h] + x);
+    };
+    uint32_t e = 8u * (uint32_t)zx;
+    if ((reinterpret_cast<uintptr_t>(in) & 15u) == 0) {
+      for (; e + 8u <= E; e += 8u * (uint32_t)g.Zc) {
+        const int4 v = __ldg(reinterpret_cast<const int4*>(in + e));
+        const uint32_t w4[4] = {(uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z, (uint32_t)v.w};
+#pragma unroll
+        for (int q = 0; q < 8; ++q) add(e + (uint32_t)q, (int16_t)(w4[q >> 1] >> (16 * (q & 1))));
+      }
+    }
+    for (; e < E; e += 8u * (uint32_t)g.Zc)
+      for (uint32_t q = e; q < e + 8u && q < E; ++q) add(q, __ldg(in + q));
+  }
+  __syncthreads();
+  for (int h = 0; h < 2; ++h) {
+    if (!scat[h]) continue;
+    const MixedCw c = p.cws[cw[h]];
+    if (!(c.harq_mode & 2) || !p.harq) continue;
+    int16_t* hq = p.harq + c.harq_off;
+    for (int i = zx; i < g.lq_len; i += g.Zc) hq[i] = (int16_t)(lq[i] >> (16 * h));
   }
 }
 
-template <bool kDegenClip>
-__global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __grid_constant__ MixedParams p) {
+template <bool kDegenClip, int kThreads, int kCap, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const __grid_constant__ MixedParams p) {
+  constexpr int kGroups = kCap / 2;       // G = floor(kCap / Zc) <= kCap / 2 (Zc >= 2)
   extern __shared__ __align__(16) uint32_t s_lq[];
-  __shared__ uint32_t s_crc[2 * kMaxGroups];
+  __shared__ uint32_t s_crc[2 * kGroups];
   __shared__ MixedGraph s_g;
-  __shared__ int4 s_grp[kMaxGroups];      // per group: B of both halves (0 when idle), CRC table offsets
-  __shared__ int s_cw[2 * kMaxGroups];    // block in each half lane, -1 when idle
+  __shared__ int4 s_grp[kGroups];         // per group: B of both halves (0 when idle), CRC table offsets
+  __shared__ int s_cw[2 * kGroups];       // block in each half lane, -1 when idle
   __shared__ int s_item;
 
   const int tid = threadIdx.x;
@@ -149,11 +209,9 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
         s_grp[g] = make_int4(cw[0] >= 0 ? p.cws[cw[0]].B : 0, cw[1] >= 0 ? p.cws[cw[1]].B : 0,
                              cw[0] >= 0 ? p.cws[cw[0]].crctype * kMaxB : 0,
                              cw[1] >= 0 ? p.cws[cw[1]].crctype * kMaxB : 0);
-      for (int i = zx; i < lq_len; i += Zc) lq[i] = 0u;
-      for (int h = 0; h < 2; ++h)
-        if (cw[h] >= 0) recover_half(p, s_g, cw[h], h, lq, zx);
     }
-    if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
+    recover_halves_mixed(p, s_g, lq, zx, active, cw, true, true);
+    if (tid < 2 * kGroups) s_crc[tid] = 0u;
     uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
     __syncthreads();
 
@@ -222,7 +280,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
       }
       // s_crc read and emits done before the lanes are refilled
       const bool any = __syncthreads_or(refill[0] || refill[1]);
-      if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
+      if (tid < 2 * kGroups) s_crc[tid] = 0u;
       if (!any) continue;   // nothing finished: the next iteration (the rows' barriers order s_crc)
       if (active && zx == 0)
         for (int h = 0; h < 2; ++h)
@@ -233,59 +291,76 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_mixed_kernel(const __
           if (!refill[h]) continue;
           cw[h] = s_cw[2 * g + h];
           itv &= h ? 0x0000FFFFu : 0xFFFF0000u;
-          if (cw[h] >= 0) {
-            recover_half(p, s_g, cw[h], h, lq, zx);
-            fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
-          }
+          if (cw[h] >= 0) fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
         }
         if (zx == 0 && (refill[0] || refill[1]))
           s_grp[g] = make_int4(cw[0] >= 0 ? p.cws[cw[0]].B : 0, cw[1] >= 0 ? p.cws[cw[1]].B : 0,
                                cw[0] >= 0 ? p.cws[cw[0]].crctype * kMaxB : 0,
                                cw[1] >= 0 ? p.cws[cw[1]].crctype * kMaxB : 0);
       }
+      recover_halves_mixed(p, s_g, lq, zx, active, cw, refill[0], refill[1]);
       if (__syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0))) break;
     }
   }
 }
 
-}  // namespace
+// Kernel instance of (degenerate clip, class).
+template <int C>
+struct MixedShape;
+template <>
+struct MixedShape<0> {
+  static constexpr int kThreads = 384, kCap = 384, kMinBlocks = 2;
+};
+template <>
+struct MixedShape<1> {
+  static constexpr int kThreads = 256, kCap = 240, kMinBlocks = 3;
+};
 
-int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream) {
-  const int smem = kThreadsTarget * kMaxCols * 4;   // largest G * (N + 2Zc) words of any (BG, Zc)
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  cudaError_t err;
-  if (degen_clip) {
-    err = cudaFuncSetAttribute(fixed_mixed_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (err != cudaSuccess) return (int)err;
-    fixed_mixed_kernel<true><<<grid, kThreadsTarget, smem, s>>>(p);
-  } else {
-    err = cudaFuncSetAttribute(fixed_mixed_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (err != cudaSuccess) return (int)err;
-    fixed_mixed_kernel<false><<<grid, kThreadsTarget, smem, s>>>(p);
-  }
-  count_launch();
-  return (int)cudaGetLastError();
+template <bool D, int C>
+constexpr auto mixed_fn() {
+  return fixed_mixed_kernel<D, MixedShape<C>::kThreads, MixedShape<C>::kCap, MixedShape<C>::kMinBlocks>;
 }
+
+template <bool D, int C>
+int mixed_op(int op, const MixedParams* p, int grid, cudaStream_t s, int* occ) {
+  const auto fn = mixed_fn<D, C>();
+  const int smem = MixedShape<C>::kCap * kMaxCols * 4;   // largest G * (N + 2Zc) words of any of its graphs
+  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (err != cudaSuccess) return (int)err;
+  if (op == 1) {
+    fn<<<grid, MixedShape<C>::kThreads, smem, s>>>(*p);
+    count_launch();
+    return (int)cudaGetLastError();
+  }
+  if (op == 2) {
+    *occ = 0;
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, fn, MixedShape<C>::kThreads, smem);
+  }
+  return 0;
+}
+
+int mixed_dispatch(int op, bool degen_clip, int cls, const MixedParams* p, int grid, void* stream, int* occ) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (cls == 1)
+    return degen_clip ? mixed_op<true, 1>(op, p, grid, s, occ) : mixed_op<false, 1>(op, p, grid, s, occ);
+  return degen_clip ? mixed_op<true, 0>(op, p, grid, s, occ) : mixed_op<false, 0>(op, p, grid, s, occ);
+}
+
+}  // namespace
 
 int bounds_read_mixed(uint32_t* out, bool reset) { return bounds_read_tu(out, reset); }
 
-int prepare_mixed(bool degen_clip) {
-  const int smem = kThreadsTarget * kMaxCols * 4;
-  cudaError_t err = degen_clip
-                        ? cudaFuncSetAttribute(fixed_mixed_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
-                        : cudaFuncSetAttribute(fixed_mixed_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  return (int)err;
+int mixed_class_capacity(int cls) { return cls == 1 ? MixedShape<1>::kCap : MixedShape<0>::kCap; }
+
+int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream, int cls) {
+  return mixed_dispatch(1, degen_clip, cls, &p, grid, stream, nullptr);
 }
 
-int occupancy_mixed(bool degen_clip) {
-  const int smem = kThreadsTarget * kMaxCols * 4;
+int prepare_mixed(bool degen_clip, int cls) { return mixed_dispatch(0, degen_clip, cls, nullptr, 0, nullptr, nullptr); }
+
+int occupancy_mixed(bool degen_clip, int cls) {
   int n = 0;
-  prepare_mixed(degen_clip);
-  if (degen_clip) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_mixed_kernel<true>, kThreadsTarget, smem);
-  } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_mixed_kernel<false>, kThreadsTarget, smem);
-  }
+  mixed_dispatch(2, degen_clip, cls, nullptr, 0, nullptr, &n);
   return n;
 }
 

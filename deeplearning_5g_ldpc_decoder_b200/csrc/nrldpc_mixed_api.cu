@@ -1,6 +1,7 @@
 // nrldpc_mixed_api.cu — host side of mixed-size batches: the plan (one block
 // queue per (BG, Zc), work items claiming them, device tables), its CUDA
-// graph, and a small autotuner over the launch shape and the work-item order.
+// graph, and a small autotuner over the CTA class of each lifting size
+// (code blocks per CTA), the launch shape and the work-item order.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -14,6 +15,8 @@
 
 namespace nrldpc {
 namespace {
+
+constexpr int kMixedAutotuneCandidates = NRLDPC_MIXED_AUTOTUNE_CANDIDATES;
 
 struct MixedPlanImpl {
   int device = 0;
@@ -29,20 +32,27 @@ struct MixedPlanImpl {
   int32_t* d_queue = nullptr;     // block queues: cb_list, then key_base, key_count
   int32_t* d_counter = nullptr;   // work-item head, then one cursor per graph
   uint32_t* d_scratch = nullptr;
+  uint32_t* d_scratch1 = nullptr;   // class-1 scratch (the classes may run at the same time)
+  int scratch1_ctas = 0;
+  cudaStream_t side = nullptr;      // class-1 launches, forked from and joined to the caller's stream
+  cudaEvent_t fork = nullptr, join = nullptr;
   size_t items_cap = 0;
   int scratch_ctas = 0;
-  MixedParams params = {};
+  MixedParams params = {};   // class-0 launch; the class-1 launch differs in items and head counter
   int order = 0;          // 0: largest work first, 1: graphs interleaved
-  int ctas_per_sm = 2;
+  int cls_mode = 0;       // 0: every graph in class 0; 1: each graph in the class that keeps more rows active
+  int ctas_per_sm = 2;    // class 0 (class 1 runs at its occupancy, 3 per SM)
+  std::vector<int> cls;   // per graph
+  int num_items_c[kMixedClasses] = {0, 0};
+  int grid_c[kMixedClasses] = {0, 0};
   int grid = 1;
   // captured graph
   cudaGraphExec_t exec = nullptr;
   const void* cap_ptrs[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaStream_t cap_stream = nullptr;
-  int cap_order = -1, cap_ctas = -1;
+  int cap_order = -1, cap_ctas = -1, cap_mode = -1;
 };
 
-constexpr uint32_t kScratchWordsPerCta = (4 * 42 + 5 * 4) * kThreadsTarget;   // BG1 layout, the larger one
 
 void free_plan(MixedPlanImpl* pl) {
   if (pl->exec) cudaGraphExecDestroy(pl->exec);
@@ -52,10 +62,29 @@ void free_plan(MixedPlanImpl* pl) {
   cudaFree(pl->d_queue);
   cudaFree(pl->d_counter);
   cudaFree(pl->d_scratch);
+  cudaFree(pl->d_scratch1);
+  if (pl->fork) cudaEventDestroy(pl->fork);
+  if (pl->join) cudaEventDestroy(pl->join);
+  if (pl->side) cudaStreamDestroy(pl->side);
   delete pl;
 }
 
-MixedGraph make_graph(int bgn, int Zc, int iLS) {
+}  // namespace
+
+uint32_t mixed_scratch_words_per_cta() {
+  uint32_t best = 0;
+  for (int bgn = 1; bgn <= 2; ++bgn) {
+    const BaseGraph& g = base_graph(bgn);
+    uint32_t planes = 0;
+    for (int r = 0; r < g.rows; ++r) planes += (uint32_t)fixed_row_planes(g.degree[r]);
+    best = std::max(best, planes * (uint32_t)kThreadsTarget);
+  }
+  return best;
+}
+
+namespace {
+
+MixedGraph make_graph(int bgn, int Zc, int iLS, int cap) {
   MixedGraph m;
   memset(&m, 0, sizeof(m));
   const BaseGraph& g = base_graph(bgn);
@@ -63,13 +92,13 @@ MixedGraph make_graph(int bgn, int Zc, int iLS) {
   m.Zc = Zc;
   m.R = g.rows;
   m.lq_len = g.cols * Zc;
-  m.G = std::max(1, kThreadsTarget / Zc);
+  m.G = std::max(1, cap / Zc);
   m.K = (bgn == 1 ? 22 : 10) * Zc;
   m.N = (bgn == 1 ? 66 : 50) * Zc;
   uint32_t off = 0;
   for (int r = 0; r < g.rows; ++r) {
     m.lr_off[r] = off;
-    off += (uint32_t)(g.degree[r] > 16 ? 5 : 4) * kThreadsTarget;
+    off += (uint32_t)fixed_row_planes(g.degree[r]) * kThreadsTarget;
     m.row_off[r] = g.row_off[r];
   }
   m.lr_off[g.rows] = off;
@@ -82,14 +111,18 @@ MixedGraph make_graph(int bgn, int Zc, int iLS) {
 // Work items for the current order: per graph, one claim per G lane pairs of
 // its blocks (a CTA refills its lanes from the graph's queue, so a claim may
 // end up with more blocks than 2G or, when other CTAs drained the queue, none).
+// The items of class-0 graphs come first, then those of class-1 graphs.
 int build_items(MixedPlanImpl* pl) {
   struct It {
     MixedItem m;
     double cost;
     int graph_rank;
   };
+  std::vector<It> all;
+  for (int c = 0; c < kMixedClasses; ++c) {
   std::vector<It> items;
   for (size_t gi = 0; gi < pl->graphs.size(); ++gi) {
+    if (pl->cls[gi] != c) continue;
     const MixedGraph& g = pl->graphs[gi];
     const BaseGraph& bg = base_graph(g.bgn);
     const int npairs_total = ((int)pl->members[gi].size() + 1) / 2;
@@ -108,8 +141,11 @@ int build_items(MixedPlanImpl* pl) {
   } else {
     std::stable_sort(items.begin(), items.end(), [](const It& a, const It& b) { return a.graph_rank < b.graph_rank; });
   }
-  std::vector<MixedItem> host(items.size());
-  for (size_t i = 0; i < items.size(); ++i) host[i] = items[i].m;
+  pl->num_items_c[c] = (int)items.size();
+  all.insert(all.end(), items.begin(), items.end());
+  }
+  std::vector<MixedItem> host(all.size());
+  for (size_t i = 0; i < all.size(); ++i) host[i] = all[i].m;
   if (host.size() > pl->items_cap) {
     cudaFree(pl->d_items);
     if (cudaMalloc(&pl->d_items, host.size() * sizeof(MixedItem)) != cudaSuccess) return NRLDPC_ERR_CUDA;
@@ -118,24 +154,58 @@ int build_items(MixedPlanImpl* pl) {
   if (cudaMemcpy(pl->d_items, host.data(), host.size() * sizeof(MixedItem), cudaMemcpyHostToDevice) != cudaSuccess)
     return NRLDPC_ERR_CUDA;
   pl->params.items = pl->d_items;
-  pl->params.num_items = (int32_t)host.size();
+  pl->params.num_items = (int32_t)pl->num_items_c[0];
   return NRLDPC_OK;
 }
 
-int configure(MixedPlanImpl* pl, int ctas_per_sm, int order) {
-  if (order != pl->order || !pl->params.items) {
+// Class of graph (BG, Zc) in cls_mode 1: the one that keeps more lifted rows
+// active per SM (class 0: 2 CTAs of floor(384/Zc) x Zc rows; class 1: 3 CTAs of
+// floor(240/Zc) x Zc rows).
+int natural_class(int Zc) {
+  const int cap1 = mixed_class_capacity(1), cap0 = mixed_class_capacity(0);
+  if (Zc > cap1) return 0;
+  return 3 * (cap1 / Zc) * Zc > 2 * (cap0 / Zc) * Zc ? 1 : 0;
+}
+
+int configure(MixedPlanImpl* pl, int ctas_per_sm, int order, int cls_mode) {
+  const bool regraph = cls_mode != pl->cls_mode || pl->cls.empty();
+  if (regraph) {
+    pl->cls_mode = cls_mode;
+    pl->cls.assign(pl->graphs.size(), 0);
+    for (size_t gi = 0; gi < pl->graphs.size(); ++gi) {
+      const int c = cls_mode == 1 ? natural_class(pl->graphs[gi].Zc) : 0;
+      pl->cls[gi] = c;
+      pl->graphs[gi].G = std::max(1, mixed_class_capacity(c) / pl->graphs[gi].Zc);
+    }
+    if (cudaMemcpy(pl->d_graphs, pl->graphs.data(), pl->graphs.size() * sizeof(MixedGraph),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+  }
+  if (regraph || order != pl->order || !pl->params.items) {
     pl->order = order;
     const int rc = build_items(pl);
     if (rc != NRLDPC_OK) return rc;
   }
-  int occ = occupancy_mixed(pl->degen);
+  int occ = occupancy_mixed(pl->degen, 0);
   if (occ < 1) occ = 1;
+  int occ1 = occupancy_mixed(pl->degen, 1);
+  if (occ1 < 1) occ1 = 1;
   pl->ctas_per_sm = std::max(1, std::min(ctas_per_sm, occ));
-  pl->grid = std::max(1, std::min(pl->params.num_items, pl->ctas_per_sm * pl->num_sms));
+  pl->grid_c[0] = std::max(0, std::min(pl->num_items_c[0], pl->ctas_per_sm * pl->num_sms));
+  pl->grid_c[1] = std::max(0, std::min(pl->num_items_c[1], occ1 * pl->num_sms));
+  pl->grid = std::max(1, pl->grid_c[0]);
+  if (pl->grid_c[1] > pl->scratch1_ctas) {
+    cudaFree(pl->d_scratch1);
+    pl->d_scratch1 = nullptr;
+    if (cudaMalloc(&pl->d_scratch1, (size_t)pl->grid_c[1] * mixed_scratch_words_per_cta() * sizeof(uint32_t)) !=
+        cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+    pl->scratch1_ctas = pl->grid_c[1];
+  }
   if (pl->grid > pl->scratch_ctas) {
     cudaFree(pl->d_scratch);
     pl->d_scratch = nullptr;
-    if (cudaMalloc(&pl->d_scratch, (size_t)pl->grid * kScratchWordsPerCta * sizeof(uint32_t)) != cudaSuccess)
+    if (cudaMalloc(&pl->d_scratch, (size_t)pl->grid * mixed_scratch_words_per_cta() * sizeof(uint32_t)) != cudaSuccess)
       return NRLDPC_ERR_CUDA;
     pl->scratch_ctas = pl->grid;
   }
@@ -144,10 +214,30 @@ int configure(MixedPlanImpl* pl, int ctas_per_sm, int order) {
 }
 
 int enqueue(MixedPlanImpl* pl, cudaStream_t s) {
-  // work-item head and every graph's queue cursor start at zero
-  if (cudaMemsetAsync(pl->params.counter, 0, sizeof(int32_t) * (1 + pl->graphs.size()), s) != cudaSuccess)
+  // both classes' work-item heads and every graph's queue cursor start at zero
+  if (cudaMemsetAsync(pl->params.counter, 0, sizeof(int32_t) * (kMixedClasses + pl->graphs.size()), s) !=
+      cudaSuccess)
     return NRLDPC_ERR_CUDA;
-  return launch_mixed(pl->params, pl->grid, pl->degen, s) == 0 ? NRLDPC_OK : NRLDPC_ERR_CUDA;
+  // The class-1 launch runs beside the class-0 one on a side stream (fork and
+  // join through events, which a CUDA graph capture records as a fork/join):
+  // its CTAs take the SMs that class-0 CTAs leave as their queue drains, so the
+  // two classes do not each pay a tail.  The graphs of the two classes are
+  // disjoint; each class has its own items, head counter and scratch.
+  const bool both = pl->grid_c[0] > 0 && pl->grid_c[1] > 0;
+  if (both && (cudaEventRecord(pl->fork, s) != cudaSuccess || cudaStreamWaitEvent(pl->side, pl->fork, 0) != cudaSuccess))
+    return NRLDPC_ERR_CUDA;
+  if (pl->grid_c[0] > 0 && launch_mixed(pl->params, pl->grid_c[0], pl->degen, s, 0) != 0) return NRLDPC_ERR_CUDA;
+  if (pl->grid_c[1] > 0) {
+    MixedParams p1 = pl->params;
+    p1.items = pl->d_items + pl->num_items_c[0];
+    p1.num_items = pl->num_items_c[1];
+    p1.counter = pl->params.counter + 1;
+    p1.scratch = pl->d_scratch1;
+    if (launch_mixed(p1, pl->grid_c[1], pl->degen, both ? pl->side : s, 1) != 0) return NRLDPC_ERR_CUDA;
+  }
+  if (both && (cudaEventRecord(pl->join, pl->side) != cudaSuccess || cudaStreamWaitEvent(s, pl->join, 0) != cudaSuccess))
+    return NRLDPC_ERR_CUDA;
+  return NRLDPC_OK;
 }
 
 int execute(MixedPlanImpl* pl, const int16_t* llr, uint8_t* bits, int32_t* status, int32_t* iters, bool use_graph,
@@ -158,12 +248,13 @@ int execute(MixedPlanImpl* pl, const int16_t* llr, uint8_t* bits, int32_t* statu
   pl->params.iters = iters;
   if (!use_graph || s == nullptr) return enqueue(pl, s);
   const void* ptrs[4] = {llr, bits, status, iters};
-  const bool same = pl->exec && s == pl->cap_stream && pl->cap_order == pl->order && pl->cap_ctas == pl->grid &&
+  const bool same = pl->exec && s == pl->cap_stream && pl->cap_order == pl->order &&
+                    pl->cap_ctas == pl->ctas_per_sm && pl->cap_mode == pl->cls_mode &&
                     memcmp(ptrs, pl->cap_ptrs, sizeof(ptrs)) == 0;
   if (!same) {
     if (pl->exec) cudaGraphExecDestroy(pl->exec);
     pl->exec = nullptr;
-    if (prepare_mixed(pl->degen) != 0) return NRLDPC_ERR_CUDA;
+    if (prepare_mixed(pl->degen, 0) != 0 || prepare_mixed(pl->degen, 1) != 0) return NRLDPC_ERR_CUDA;
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return NRLDPC_ERR_CUDA;
     const int rc = enqueue(pl, s);
@@ -177,10 +268,12 @@ int execute(MixedPlanImpl* pl, const int16_t* llr, uint8_t* bits, int32_t* statu
     memcpy(pl->cap_ptrs, ptrs, sizeof(ptrs));
     pl->cap_stream = s;
     pl->cap_order = pl->order;
-    pl->cap_ctas = pl->grid;
+    pl->cap_ctas = pl->ctas_per_sm;
+    pl->cap_mode = pl->cls_mode;
   }
   if (cudaGraphLaunch(pl->exec, s) != cudaSuccess) return NRLDPC_ERR_CUDA;
-  count_launch();   // the kernel node of the replayed graph
+  if (pl->grid_c[0] > 0) count_launch();   // the kernel nodes of the replayed graph
+  if (pl->grid_c[1] > 0) count_launch();
   return NRLDPC_OK;
 }
 
@@ -201,8 +294,14 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
   }
   MixedPlanImpl* pl = new MixedPlanImpl();
   cudaGetDevice(&pl->device);
+  if (cudaStreamCreateWithFlags(&pl->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&pl->join, cudaEventDisableTiming) != cudaSuccess) {
+    free_plan(pl);
+    return NRLDPC_ERR_CUDA;
+  }
   if (cudaDeviceGetAttribute(&pl->num_sms, cudaDevAttrMultiProcessorCount, pl->device) != cudaSuccess) {
-    delete pl;
+    free_plan(pl);
     return NRLDPC_ERR_CUDA;
   }
   pl->num_cw = num_blocks;
@@ -212,18 +311,18 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
   for (int i = 0; i < num_blocks; ++i) {
     CodeParams cp;
     if (derive_params(blocks[i].cfg, &cp, true) != 0) {
-      delete pl;
+      free_plan(pl);
       return NRLDPC_ERR_CONFIG;
     }
     if (cp.harq_on || blocks[i].llr_offset < 0 || blocks[i].bits_offset < 0) {
-      delete pl;
+      free_plan(pl);
       return NRLDPC_ERR_ARG;
     }
     const auto key = std::make_pair(cp.bgn, cp.Zc);
     auto itg = gidx.find(key);
     if (itg == gidx.end()) {
       itg = gidx.emplace(key, (int)pl->graphs.size()).first;
-      pl->graphs.push_back(make_graph(cp.bgn, cp.Zc, cp.iLS));
+      pl->graphs.push_back(make_graph(cp.bgn, cp.Zc, cp.iLS, mixed_class_capacity(0)));
       pl->members.emplace_back();
     }
     pl->members[itg->second].push_back(i);
@@ -247,7 +346,7 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
   p.fill = dc->filling_bit_value;
   p.max_llr = dc->max_llr;
   p.min_llr = dc->min_llr;
-  p.scratch_words = kScratchWordsPerCta;
+  p.scratch_words = mixed_scratch_words_per_cta();
   for (int b = 0; b < 2; ++b) {
     const BaseGraph& g = base_graph(b + 1);
     for (int r = 0; r < g.rows; ++r) {
@@ -256,7 +355,7 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
     }
     p.weights_T[b] = 0;
     if (dc->algo == 2 && device_trained_table(b + 1, &p.weights[b], &p.weights_T[b]) != NRLDPC_OK) {
-      delete pl;
+      free_plan(pl);
       return NRLDPC_ERR_CUDA;
     }
   }
@@ -274,7 +373,7 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
   if (device_crc_table(&p.crc_tab) != NRLDPC_OK ||
       cudaMalloc(&pl->d_graphs, pl->graphs.size() * sizeof(MixedGraph)) != cudaSuccess ||
       cudaMalloc(&pl->d_cws, pl->cws.size() * sizeof(MixedCw)) != cudaSuccess ||
-      cudaMalloc(&pl->d_counter, sizeof(int32_t) * (1 + ng)) != cudaSuccess ||
+      cudaMalloc(&pl->d_counter, sizeof(int32_t) * (kMixedClasses + ng)) != cudaSuccess ||
       cudaMalloc(&pl->d_queue, sizeof(int32_t) * queue.size()) != cudaSuccess ||
       cudaMemcpy(pl->d_graphs, pl->graphs.data(), pl->graphs.size() * sizeof(MixedGraph), cudaMemcpyHostToDevice) !=
           cudaSuccess ||
@@ -287,11 +386,12 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
   p.cb_list = pl->d_queue;
   p.key_base = pl->d_queue + (queue.size() - 2 * ng);
   p.key_count = pl->d_queue + (queue.size() - ng);
-  p.key_cursor = pl->d_counter + 1;
+  p.key_cursor = pl->d_counter + kMixedClasses;
   p.graphs = pl->d_graphs;
   p.cws = pl->d_cws;
   p.counter = pl->d_counter;
-  const int rc = configure(pl, 2, 0);
+  pl->cls_mode = -1;   // configure() assigns the classes and uploads the graph tables
+  const int rc = configure(pl, 2, 0, 1);
   if (rc != NRLDPC_OK) {
     free_plan(pl);
     return rc;
@@ -307,18 +407,28 @@ int32_t nrldpc_mixed_plan_execute(void* plan, const int16_t* d_llr, uint8_t* d_b
                  reinterpret_cast<cudaStream_t>(stream));
 }
 
+// Autotuner candidates: (class mode, class-0 CTAs per SM, work order).
+constexpr int kCand[kMixedAutotuneCandidates][3] = {{1, 2, 0}, {1, 1, 0}, {1, 2, 1}, {1, 1, 1},
+                                                    {0, 2, 0}, {0, 1, 0}, {0, 2, 1}, {0, 1, 1}};
+
+int32_t nrldpc_mixed_plan_select(void* plan, int32_t candidate) {
+  if (!plan || candidate < 0 || candidate >= kMixedAutotuneCandidates) return NRLDPC_ERR_ARG;
+  const int* c = kCand[candidate];
+  return configure(static_cast<MixedPlanImpl*>(plan), c[1], c[2], c[0]);
+}
+
 int32_t nrldpc_mixed_plan_autotune(void* plan, const int16_t* d_llr, uint8_t* d_bits, int32_t* d_status,
                                    int32_t* d_iterations, float* ms_out, void* stream) {
   if (!plan || !d_llr) return NRLDPC_ERR_ARG;
   MixedPlanImpl* pl = static_cast<MixedPlanImpl*>(plan);
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const int cand[4][2] = {{2, 0}, {1, 0}, {2, 1}, {1, 1}};   // (CTAs per SM, work order)
+  const auto& cand = kCand;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return NRLDPC_ERR_CUDA;
   int best = 0;
   float best_ms = 1e30f;
-  for (int c = 0; c < 4; ++c) {
-    if (configure(pl, cand[c][0], cand[c][1]) != NRLDPC_OK) return NRLDPC_ERR_CUDA;
+  for (int c = 0; c < kMixedAutotuneCandidates; ++c) {
+    if (configure(pl, cand[c][1], cand[c][2], cand[c][0]) != NRLDPC_OK) return NRLDPC_ERR_CUDA;
     if (execute(pl, d_llr, d_bits, d_status, d_iterations, false, s) != NRLDPC_OK) return NRLDPC_ERR_CUDA;
     cudaEventRecord(e0, s);
     for (int r = 0; r < 3; ++r)
@@ -336,7 +446,7 @@ int32_t nrldpc_mixed_plan_autotune(void* plan, const int16_t* d_llr, uint8_t* d_
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (configure(pl, cand[best][0], cand[best][1]) != NRLDPC_OK) return NRLDPC_ERR_CUDA;
+  if (configure(pl, cand[best][1], cand[best][2], cand[best][0]) != NRLDPC_OK) return NRLDPC_ERR_CUDA;
   return best;
 }
 

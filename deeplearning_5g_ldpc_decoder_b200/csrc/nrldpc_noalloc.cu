@@ -128,6 +128,8 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
   p.symbols = cp.symbols;
   p.c0 = cp.c0;
   p.max_it = dc->max_iterations;
+  p.rr_scatter = cp.E <= cp.Nv;
+  p.qm_magic = qm_magic(cp.Qm);
   p.harq_on = cp.harq_on;
   p.fill = dc->filling_bit_value;
   p.max_llr = dc->max_llr;
@@ -175,7 +177,7 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
   uint32_t off = 0;
   for (int r = 0; r < g.rows; ++r) {
     p.lr_off[r] = off;
-    off += (uint32_t)(g.degree[r] > 16 ? 5 : 4) * (uint32_t)kThreadsTarget;
+    off += (uint32_t)fixed_row_planes(g.degree[r]) * (uint32_t)kThreadsTarget;
   }
   p.lr_off[g.rows] = off;
   p.scratch_words = off;
@@ -194,6 +196,7 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
   const int grid = std::max(1, std::min({p.num_items, occ * nd->num_sms, fit}));
   p.llr = d_llr;
   p.llr_stride = llr_stride;
+  p.rr_vec = (reinterpret_cast<uintptr_t>(d_llr) % 16 == 0) && (llr_stride % 8 == 0);
   p.bits = d_bits;
   p.bits_stride = bits_stride;
   p.status = d_status;

@@ -34,7 +34,6 @@ namespace {
 
 constexpr int kCbBitsStride = kMaxB / 8;   // 1056 bytes of hard bits per code block
 constexpr int kKeys = 128;                 // tb_graph_key range
-constexpr uint32_t kScratchWordsPerCta = (4 * 42 + 5 * 4) * kThreadsTarget;   // as the mixed plans
 constexpr int kSegThreads = 1024;
 
 struct SegParams {
@@ -337,7 +336,7 @@ MixedGraph tb_make_graph(int bgn, int Zc, int iLS) {
   uint32_t off = 0;
   for (int r = 0; r < g.rows; ++r) {
     m.lr_off[r] = off;
-    off += (uint32_t)(g.degree[r] > 16 ? 5 : 4) * kThreadsTarget;
+    off += (uint32_t)fixed_row_planes(g.degree[r]) * kThreadsTarget;
     m.row_off[r] = g.row_off[r];
   }
   m.lr_off[g.rows] = off;
@@ -386,7 +385,7 @@ int engine_lanes(TbEngine* e, int n) {
         cudaMalloc(&l->d_cb_bits, (size_t)max_cbs * kCbBitsStride) == cudaSuccess &&
         cudaMalloc(&l->d_cb_status, (size_t)max_cbs * sizeof(int32_t)) == cudaSuccess &&
         cudaMalloc(&l->d_cb_iters, (size_t)max_cbs * sizeof(int32_t)) == cudaSuccess &&
-        cudaMalloc(&l->d_scratch, (size_t)e->grid * kScratchWordsPerCta * sizeof(uint32_t)) == cudaSuccess &&
+        cudaMalloc(&l->d_scratch, (size_t)e->grid * mixed_scratch_words_per_cta() * sizeof(uint32_t)) == cudaSuccess &&
         cudaMemset(l->d_num_items, 0, 2 * sizeof(int32_t)) == cudaSuccess;
     if (!ok) {
       lane_free(l);
@@ -579,7 +578,7 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
   p.graphs = e->d_graphs;
   p.num_items = 0;
   p.crc_tab = e->d_crc_tab;
-  p.scratch_words = kScratchWordsPerCta;
+  p.scratch_words = mixed_scratch_words_per_cta();
   p.max_it = dc->max_iterations;
   p.fill = dc->filling_bit_value;
   p.max_llr = dc->max_llr;

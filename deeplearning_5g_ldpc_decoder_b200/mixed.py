@@ -13,6 +13,14 @@ from . import capi
 from .capi import LdpcInConfig
 
 
+# nrldpc_mixed_plan_autotune's candidates, in its order (NRLDPC_MIXED_AUTOTUNE_CANDIDATES).
+AUTOTUNE_CANDIDATES = 8
+AUTOTUNE_NAMES = [f"{cls}, {ctas} CTA/SM, {order}"
+                  for cls in ("right-sized CTAs", "384-thread CTAs")
+                  for order in ("largest-first", "interleaved")
+                  for ctas in (2, 1)]
+
+
 class Block(ctypes.Structure):
     """nrldpc_block_t."""
 
@@ -30,6 +38,8 @@ def _declare(lib):
     lib.nrldpc_mixed_plan_execute.restype = i32
     lib.nrldpc_mixed_plan_autotune.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     lib.nrldpc_mixed_plan_autotune.restype = i32
+    lib.nrldpc_mixed_plan_select.argtypes = [vp, i32]
+    lib.nrldpc_mixed_plan_select.restype = i32
     lib.nrldpc_mixed_plan_destroy.argtypes = [vp]
     lib.nrldpc_mixed_plan_destroy.restype = i32
     lib._mixed_declared = True
@@ -98,7 +108,7 @@ class MixedPlan:
 
     def autotune(self, llr_arena: torch.Tensor, out=None):
         bits, status, iters = out if out is not None else self.outputs()
-        ms = (ctypes.c_float * 4)()
+        ms = (ctypes.c_float * AUTOTUNE_CANDIDATES)()
         stream = torch.cuda.current_stream(self.device).cuda_stream
         with torch.cuda.device(self.device):
             best = self.lib.nrldpc_mixed_plan_autotune(self._plan, ctypes.c_void_p(llr_arena.data_ptr()),
@@ -108,6 +118,13 @@ class MixedPlan:
         if best < 0:
             raise RuntimeError(f"nrldpc_mixed_plan_autotune failed: {best}")
         return best, list(ms)
+
+    def select(self, candidate: int) -> None:
+        """Use autotuner candidate `candidate` (AUTOTUNE_NAMES order) without timing."""
+        with torch.cuda.device(self.device):
+            rc = self.lib.nrldpc_mixed_plan_select(self._plan, int(candidate))
+        if rc != 0:
+            raise RuntimeError(f"nrldpc_mixed_plan_select failed: {rc}")
 
     def block_bits(self, bits: torch.Tensor, i: int) -> torch.Tensor:
         return bits[self.bits_offsets[i]: self.bits_offsets[i] + self.nbytes[i]]

@@ -274,13 +274,23 @@ int32_t nrldpc_mixed_plan_execute(void *plan, const int16_t *d_llr, uint8_t *d_b
                                   int32_t *d_status, int32_t *d_iterations,
                                   int32_t use_graph, void *stream);
 
-/* Time the plan's candidate launch shapes (CTAs per SM 2 or 1) x work orders
- * (largest items first / graphs interleaved) on the given data, keep the
- * fastest and return its index (0..3); ms_out (nullable) receives the four
- * mean times in ms.  Synchronises the stream. */
+/* Time the plan's candidates on the given data, keep the fastest and return
+ * its index; ms_out (nullable) receives NRLDPC_MIXED_AUTOTUNE_CANDIDATES mean
+ * times in ms.  Candidate k: code blocks per CTA (k < 4: each lifting size in
+ * the CTA class that keeps more lifted rows active, 384-thread CTAs or
+ * 256-thread CTAs with at most 240 active, three per SM; k >= 4: every size in
+ * 384-thread CTAs) x CTAs per SM of the 384-thread class (2 for even k, 1 for
+ * odd) x work order (largest items first for k mod 4 < 2, graphs interleaved
+ * otherwise).  Synchronises the stream. */
+#define NRLDPC_MIXED_AUTOTUNE_CANDIDATES 8
 int32_t nrldpc_mixed_plan_autotune(void *plan, const int16_t *d_llr, uint8_t *d_bits,
                                    int32_t *d_status, int32_t *d_iterations,
                                    float *ms_out, void *stream);
+
+/* Select autotuner candidate `candidate` (0 .. NRLDPC_MIXED_AUTOTUNE_CANDIDATES-1,
+ * the same numbering) without timing anything.  A new plan starts at
+ * candidate 0.  Returns 0, -4 for an unknown candidate, -1 on a CUDA error. */
+int32_t nrldpc_mixed_plan_select(void *plan, int32_t candidate);
 
 int32_t nrldpc_mixed_plan_destroy(void *plan);
 

@@ -42,7 +42,7 @@ def test_mixed_batch_bit_exact_per_block(oracle, cuda, row):
         conv += es == 0
     assert 0 < conv < len(cfgs)      # a mix of converging and failing blocks
     best, ms = plan.autotune(arena)
-    assert 0 <= best < 4 and all(m > 0 for m in ms)
+    assert 0 <= best < 8 and len(ms) == 8 and all(m > 0 for m in ms)
     bits3, status3, _ = plan.decode(arena, use_graph=False)
     torch.cuda.synchronize()
     assert torch.equal(bits3, bits) and torch.equal(status3, status)
@@ -117,4 +117,46 @@ def test_config3_full_batch_every_block_matches_oracle(cuda):
     assert len(bad_status) == 0 and len(bad_bits) == 0, (bad_status[:10], bad_bits[:10])
     conv = int((est == 0).sum())
     assert 0.5 * n < conv < n and len(set(eit.tolist())) >= 5
+    plan.close()
+
+
+def test_right_sized_ctas_match_384_thread_ctas_and_oracle(oracle, cuda):
+    """Lifting sizes where 384-thread CTAs leave threads idle (104 .. 240) go to
+    256-thread CTAs (at most 240 active lifted rows, three per SM) under the
+    right-sized candidates; the results must not depend on the CTA class: both
+    equal the oracle block by block."""
+    import ctypes
+
+    from deeplearning_5g_ldpc_decoder_b200 import capi
+
+    lib = capi.load_library()
+    want_zc = {104, 112, 120, 208, 224, 240, 192, 384, 26, 13}
+    pool = random_mixed_configs(20000, seed=41, rvs=(0,))
+    cfgs, seen = [], {}
+    for c in pool:
+        out = capi.LdpcConfig()
+        assert lib.gen_ldpc_parameters(ctypes.byref(out), ctypes.byref(capi.make_in_config(*c, 0))) == 0
+        if out.Zc in want_zc and seen.get((c[0], out.Zc), 0) < 24:
+            seen[(c[0], out.Zc)] = seen.get((c[0], out.Zc), 0) + 1
+            cfgs.append(c)
+    assert {z for _, z in seen} >= {208, 224, 240}
+    cfgs, llrs = _build(oracle, len(cfgs), seed=9, noise_db=-6.0, cfgs=cfgs)
+    row = [1, 8, 22936, 0, 1280, 32767, -32767]
+    plan = MixedPlan(cfgs, row, device=cuda)
+    arena = plan.pack_llrs(llrs)
+    res = {}
+    for cand in (0, 3, 4, 7):
+        plan.select(cand)
+        bits, status, iters = plan.decode(arena, use_graph=cand % 2 == 0)
+        torch.cuda.synchronize()
+        res[cand] = (bits.clone(), status.clone(), iters.clone())
+    for cand in (3, 4, 7):
+        assert all(torch.equal(a, b) for a, b in zip(res[0], res[cand])), cand
+    b, st, it = (t.cpu().numpy() for t in res[0])     # (bits, status, iterations)
+    for i, c in enumerate(cfgs):
+        es, eb, ei, _ = oracle.decode(llrs[i].numpy(), in_config(*c, 0), dec_cfg(row))
+        assert (st[i], it[i]) == (es, ei), (i, c)
+        assert np.array_equal(b[plan.bits_offsets[i]: plan.bits_offsets[i] + plan.nbytes[i]], eb), (i, c)
+    with pytest.raises(RuntimeError):
+        plan.select(8)
     plan.close()

@@ -116,3 +116,42 @@ def test_shard_helpers_single_process():
     assert max_over_ranks(2.5) == 2.5 and sum_over_ranks(3) == 3.0
     with pytest.raises(ValueError):
         strong_shard(10, 2, 2)
+
+
+_PROBE = '''
+import datetime, json, os, sys
+sys.path.insert(0, {repo!r})
+import torch.distributed as dist
+from deeplearning_5g_ldpc_decoder_b200.shard import max_over_ranks, sum_over_ranks
+rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
+dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+ms = max_over_ranks(10.0 + rank, dist)
+units = sum_over_ranks(8192, dist)
+dist.barrier()
+if rank == 0:
+    print(json.dumps({{"n_gpus": world, "ms_per_step": ms, "units": units, "argv": sys.argv[1:]}}), flush=True)
+dist.destroy_process_group()
+'''
+
+
+def test_launch_ranks_starts_world_size_ranks(tmp_path):
+    """`bench.py --gpus N` outside a launcher re-runs itself under
+    torch.distributed.run through shard.launch_ranks: two gloo ranks on CPU
+    start, combine a time (max) and a count (sum) like bench.py does, and rank 0
+    prints one line with n_gpus 2."""
+    import json
+    import subprocess
+
+    from deeplearning_5g_ldpc_decoder_b200.shard import torchrun_command
+
+    script = tmp_path / "probe.py"
+    script.write_text(_PROBE.format(repo=REPO))
+    cmd = torchrun_command(2, str(script), ["--gpus", "2"], _free_port(), timeout_s=120)
+    assert cmd[:3] == ["timeout", "-k", "60"] and "--nproc-per-node=2" in cmd
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    out = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=180)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    rec = json.loads(lines[0])
+    assert rec == {"n_gpus": 2, "ms_per_step": 11.0, "units": 16384.0, "argv": ["--gpus", "2"]}
