@@ -128,4 +128,26 @@ __device__ __forceinline__ uint32_t crc_term(const DecodeParams& p, int i) {
   return NRLDPC_INBOUNDS(p.B - 1 - i, kMaxB, kBoundsCrc) ? __ldg(p.crc_tab + (p.B - 1 - i)) : 0u;
 }
 
+// Group index k / Bp of the hard-decision loops without an integer divide:
+// the multiply-high by magic = ceil(2^32 / Bp) is exact while
+// k * (magic * Bp - 2^32) < 2^32.  Bp = roundup32(K) <= 8480 and
+// k < G * Bp <= 14400 (G = floor(384 / Zc), K <= 22 Zc), so the product
+// stays below 1.3e8.
+__device__ __forceinline__ uint32_t bp_magic(int Bp) { return 0xFFFFFFFFu / (uint32_t)Bp + 1u; }
+__device__ __forceinline__ int div_bp(int k, uint32_t magic) { return (int)__umulhi((uint32_t)k, magic); }
+
+// Per-layer descriptor staged in shared memory at kernel start, one 16-byte
+// load per layer instead of several dynamically indexed parameter reads:
+// x = the layer's word offset in the CTA's message scratch,
+// y = first edge | degree << 16 | (five message planes) << 24,
+// z = the layer's packed alpha | beta << 16 (unused with per-iteration weights).
+__device__ __forceinline__ uint4 row_descriptor(const DecodeParams& p, int r) {
+  const uint32_t e0 = p.row_off[r], deg = (uint32_t)p.row_off[r + 1] - e0;
+  const uint32_t five = p.lr_off[r + 1] - p.lr_off[r] > 4u * kThreadsTarget ? 1u : 0u;
+  return make_uint4(p.lr_off[r], e0 | (deg << 16) | (five << 24), p.w_inline[r], 0u);
+}
+__device__ __forceinline__ int row_e0(uint32_t y) { return (int)(y & 0xFFFFu); }
+__device__ __forceinline__ int row_deg(uint32_t y) { return (int)((y >> 16) & 0xFFu); }
+__device__ __forceinline__ bool row_five(uint32_t y) { return (y >> 24) != 0u; }
+
 }  // namespace nrldpc

@@ -33,6 +33,9 @@
 //    item has finished.
 //  * Each row's compressed message words are loaded while the row before it
 //    computes (load_row_msg), hiding their L2 latency.
+//  * Per-layer descriptors (scratch offset, first edge, degree, plane count,
+//    alpha|beta) are staged in shared memory at kernel start: one 16-byte
+//    shared load per layer replaces six dynamically indexed parameter reads.
 //  * CRC early termination runs every iteration inside the kernel: each hard
 //    bit i contributes x^(B-1-i+W) mod g(x) (a precomputed table), the
 //    contributions are XOR-reduced with warp reductions and shared atomics.
@@ -81,9 +84,10 @@ __device__ void emit_block(const DecodeParams& p, const uint32_t* lq, int zx, in
 // Hard decisions + CRC remainder of both halves of every group into s_crc
 // (zero for a block whose CRC passes).  Warp-uniform trip count: Bp and the
 // block size are multiples of 32.
-__device__ __forceinline__ void crc_pass(const DecodeParams& p, const uint32_t* s_lq, uint32_t* s_crc, int Bp) {
+__device__ __forceinline__ void crc_pass(const DecodeParams& p, const uint32_t* s_lq, uint32_t* s_crc, int Bp,
+                                         uint32_t magic) {
   for (int k = threadIdx.x; k < p.G * Bp; k += blockDim.x) {
-    const int gg = k / Bp;
+    const int gg = div_bp(k, magic);
     const int i = k - gg * Bp;
     uint32_t r0 = 0u, r1 = 0u;
     if (i < p.B) {
@@ -157,7 +161,9 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
   extern __shared__ __align__(16) uint32_t s_lq[];        // [G][lq_len] int16x2
   __shared__ uint32_t s_crc[2 * kMaxGroups];
   __shared__ uint2 s_edges[kMaxNnz];   // per-edge (col*Zc*4, (V mod Zc)*4), read with warp-uniform indices
+  __shared__ uint4 s_rows[kMaxRows];   // per-layer descriptors (row_descriptor)
   for (int e = threadIdx.x; e < kMaxNnz; e += blockDim.x) s_edges[e] = p.edge_cs4[e];
+  for (int r = threadIdx.x; r < p.R; r += blockDim.x) s_rows[r] = row_descriptor(p, r);
 
   const int tid = threadIdx.x;
   const int g = tid / p.Zc;
@@ -171,6 +177,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
       !NRLDPC_INBOUNDS(blockDim.x - 1u, kThreadsTarget, kBoundsScratch))
     return;
   const int Bp = (p.B + 31) & ~31;
+  const uint32_t bpm = bp_magic(Bp);
   const uint32_t zx4 = 4u * (uint32_t)zx;
   const uint32_t zxm4 = zx4 - 4u * (uint32_t)p.Zc;     // wraps: min(zx4+s, zxm4+s) = ((zx+V) mod Zc)*4
   const uint32_t gb4 = 4u * (uint32_t)((active ? g : 0) * p.lq_len);
@@ -198,26 +205,26 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
       for (int row = 0; run && row < p.R; ++row) {
         if (active) {
           const RowMsg cur = nxt;
+          const uint4 d = s_rows[row];
           const int rn = row + 1 < p.R ? row + 1 : 0;
-          nxt = load_row_msg(scratch + p.lr_off[rn] + tid, p.lr_off[rn + 1] - p.lr_off[rn] > 4u * kThreadsTarget);
-          const int e0 = p.row_off[row];
-          const int deg = p.row_off[row + 1] - e0;
+          const uint2 dn = *reinterpret_cast<const uint2*>(&s_rows[rn]);
+          nxt = load_row_msg(scratch + dn.x + tid, row_five(dn.y));
           uint32_t ab0, ab1;
           if (p.weights_T > 0) {
             ab0 = __ldg(p.weights + (min((int)(itv & 0xFFFFu), p.weights_T - 1) * p.R + row));
             ab1 = __ldg(p.weights + (min((int)(itv >> 16), p.weights_T - 1) * p.R + row));
           } else {
-            ab0 = ab1 = p.w_inline[row];
+            ab0 = ab1 = d.z;
           }
-          layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, lq_limit,
-                                           e0, (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
+          layer_dispatch<kDegenClip, true>(row_deg(d.y), p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
+                                           lq_limit, row_e0(d.y), (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
                                            (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, cur, fresh,
-                                           scratch + p.lr_off[row] + tid);
+                                           scratch + d.x + tid);
         }
         __syncthreads();
       }
       fresh = 0u;
-      if (run) crc_pass(p, s_lq, s_crc, Bp);
+      if (run) crc_pass(p, s_lq, s_crc, Bp, bpm);
       __syncthreads();
       bool fin[2] = {false, false};
       if (active) {
@@ -303,23 +310,22 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
         for (int row = 0; row < p.R; ++row) {
           if (active) {
             const RowMsg cur = nxt;
+            const uint4 d = s_rows[row];
             const int rn = row + 1 < p.R ? row + 1 : 0;
-            nxt = load_row_msg(scratch + p.lr_off[rn] + tid, p.lr_off[rn + 1] - p.lr_off[rn] > 4u * kThreadsTarget);
-            const int e0 = p.row_off[row];
-            const int deg = p.row_off[row + 1] - e0;
-            const uint32_t ab = p.weights_T > 0 ? __ldg(p.weights + (min(it, p.weights_T - 1) * p.R + row))
-                                                : p.w_inline[row];
+            const uint2 dn = *reinterpret_cast<const uint2*>(&s_rows[rn]);
+            nxt = load_row_msg(scratch + dn.x + tid, row_five(dn.y));
+            const uint32_t ab = p.weights_T > 0 ? __ldg(p.weights + (min(it, p.weights_T - 1) * p.R + row)) : d.z;
             const int32_t alpha = (int32_t)(int16_t)(ab & 0xFFFFu);
             const int32_t beta = ((int32_t)ab) >> 16;
-            layer_dispatch<kDegenClip, true>(deg, p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4, lq_limit, e0,
-                                             alpha, beta,
-                                             alpha, beta, cur, it == 0 ? 0xFFFFFFFFu : 0u, scratch + p.lr_off[row] + tid);
+            layer_dispatch<kDegenClip, true>(row_deg(d.y), p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
+                                             lq_limit, row_e0(d.y), alpha, beta, alpha, beta, cur,
+                                             it == 0 ? 0xFFFFFFFFu : 0u, scratch + d.x + tid);
           }
           __syncthreads();
         }
 
         // ---- hard decisions + CRC of every code block in the CTA ----
-        crc_pass(p, s_lq, s_crc, Bp);
+        crc_pass(p, s_lq, s_crc, Bp, bpm);
         __syncthreads();
         bool pass0 = false, pass1 = false;
         if (active) {

@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
   // lr_off[R]) lies inside its scratch
   if (!NRLDPC_INBOUNDS(p.lr_off[p.R] - 1u, p.scratch_words, kBoundsScratch)) return;
   const int Bp = (p.B + 31) & ~31;
+  const uint32_t bpm = bp_magic(Bp);
 
   // Work items: fixed (item += grid) or, with a queue cursor, taken from the
   // device queue so CTAs that run faster take more (see the fixed-point kernel).
@@ -302,7 +303,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
         __syncthreads();
       }
       for (int k = tid; k < p.G * Bp; k += blockDim.x) {
-        const int gg = k / Bp;
+        const int gg = div_bp(k, bpm);
         const int i = k - gg * Bp;
         uint32_t r = 0u;
         if (i < p.B && s_lqf[gg * p.lq_len + i] < 0.0f) r = crc_term(p, i);

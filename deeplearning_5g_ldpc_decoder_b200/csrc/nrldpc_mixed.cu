@@ -220,6 +220,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
     const uint32_t zxm4 = zx4 - 4u * (uint32_t)Zc;
     const uint32_t gb4 = 4u * (uint32_t)((active ? g : 0) * lq_len);
     const int Bp = (s_g.K + 31) & ~31;   // every block's B <= K
+    const uint32_t bpm = bp_magic(Bp);
     RowMsg nxt{};
     for (;;) {
       const bool run = p.max_it > 0;   // max_iterations == 0: rate recovery only, status 1
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
       fresh = 0u;
       // Hard decisions + CRC of both halves of every group (each with its own B and CRC type).
       for (int k = tid; run && k < G * Bp; k += blockDim.x) {
-        const int gg = k / Bp;
+        const int gg = div_bp(k, bpm);
         const int i = k - gg * Bp;
         const int4 gr = s_grp[gg];
         uint32_t r0 = 0u, r1 = 0u;
