@@ -81,28 +81,42 @@ __device__ void emit_block(const DecodeParams& p, const uint32_t* lq, int zx, in
   }
 }
 
+// XOR of the warp's partial remainders of slot gg into s_crc.
+__device__ __forceinline__ void crc_flush(uint32_t* s_crc, int gg, uint32_t r0, uint32_t r1) {
+  r0 = __reduce_xor_sync(0xFFFFFFFFu, r0);
+  r1 = __reduce_xor_sync(0xFFFFFFFFu, r1);
+  if ((threadIdx.x & 31) == 0) {
+    if (r0) atomicXor(&s_crc[2 * gg], r0);
+    if (r1) atomicXor(&s_crc[2 * gg + 1], r1);
+  }
+}
+
 // Hard decisions + CRC remainder of both halves of every group into s_crc
-// (zero for a block whose CRC passes).  Warp-uniform trip count: Bp and the
-// block size are multiples of 32.
-__device__ __forceinline__ void crc_pass(const DecodeParams& p, const uint32_t* s_lq, uint32_t* s_crc, int Bp,
-                                         uint32_t magic) {
+// (zero for a block whose CRC passes).  Bp and the block size are multiples
+// of 32, so a warp's 32 consecutive k share one slot gg and one trip count:
+// each thread XORs its terms while gg stays the same and the warp reduces
+// once per slot (once per pass when G = 1).
+__device__ __forceinline__ void crc_pass(const DecodeParams& p, const uint32_t* s_lq, uint32_t* s_crc) {
+  const int Bp = (p.B + 31) & ~31;
+  const uint32_t magic = bp_magic(Bp);
+  uint32_t r0 = 0u, r1 = 0u;
+  int cur = -1;
   for (int k = threadIdx.x; k < p.G * Bp; k += blockDim.x) {
     const int gg = div_bp(k, magic);
+    if (gg != cur) {
+      if (cur >= 0) crc_flush(s_crc, cur, r0, r1);
+      r0 = r1 = 0u;
+      cur = gg;
+    }
     const int i = k - gg * Bp;
-    uint32_t r0 = 0u, r1 = 0u;
     if (i < p.B) {
       const uint32_t w = s_lq[gg * p.lq_len + i];
       const uint32_t tv = crc_term(p, i);
-      r0 = (w & 0x8000u) ? tv : 0u;
-      r1 = (w & 0x80000000u) ? tv : 0u;
-    }
-    r0 = __reduce_xor_sync(0xFFFFFFFFu, r0);
-    r1 = __reduce_xor_sync(0xFFFFFFFFu, r1);
-    if ((threadIdx.x & 31) == 0) {
-      if (r0) atomicXor(&s_crc[2 * gg], r0);
-      if (r1) atomicXor(&s_crc[2 * gg + 1], r1);
+      r0 ^= (w & 0x8000u) ? tv : 0u;
+      r1 ^= (w & 0x80000000u) ? tv : 0u;
     }
   }
+  if (cur >= 0) crc_flush(s_crc, cur, r0, r1);
 }
 
 // Rate recovery into the halves of the group's LQ words selected by r0 / r1
@@ -176,8 +190,6 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
   if (!NRLDPC_INBOUNDS(p.lr_off[p.R] - 1u, p.scratch_words, kBoundsScratch) ||
       !NRLDPC_INBOUNDS(blockDim.x - 1u, kThreadsTarget, kBoundsScratch))
     return;
-  const int Bp = (p.B + 31) & ~31;
-  const uint32_t bpm = bp_magic(Bp);
   const uint32_t zx4 = 4u * (uint32_t)zx;
   const uint32_t zxm4 = zx4 - 4u * (uint32_t)p.Zc;     // wraps: min(zx4+s, zxm4+s) = ((zx+V) mod Zc)*4
   const uint32_t gb4 = 4u * (uint32_t)((active ? g : 0) * p.lq_len);
@@ -186,19 +198,25 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
   if constexpr (kRefill) {
     __shared__ int s_cw[2 * kMaxGroups];   // block in each half lane, -1 when idle
     __shared__ int s_base;
+    // The half lanes' blocks live in s_cw, not in registers: the layer loop
+    // needs every register it can get.
     if (tid == 0) s_base = atomicAdd(p.cursor, 2 * p.G);
     __syncthreads();
-    int cw[2] = {-1, -1};
-    if (active) {
-      cw[0] = s_base + 2 * g < p.num_cw ? s_base + 2 * g : -1;
-      cw[1] = s_base + 2 * g + 1 < p.num_cw ? s_base + 2 * g + 1 : -1;
-      if (!p.rr_scatter) recover_halves(p, lq, zx, cw[0], cw[1], true, true);
+    if (active && zx == 0) {
+      s_cw[2 * g] = s_base + 2 * g < p.num_cw ? s_base + 2 * g : -1;
+      s_cw[2 * g + 1] = s_base + 2 * g + 1 < p.num_cw ? s_base + 2 * g + 1 : -1;
     }
-    if (p.rr_scatter) recover_scatter(p, lq, zx, active, cw[0], cw[1], true, true);
+    __syncthreads();
+    bool idle;
+    {
+      const int c0 = active ? s_cw[2 * g] : -1, c1 = active ? s_cw[2 * g + 1] : -1;
+      if (active && !p.rr_scatter) recover_halves(p, lq, zx, c0, c1, true, true);
+      if (p.rr_scatter) recover_scatter(p, lq, zx, active, c0, c1, true, true);
+      if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
+      idle = __syncthreads_and(!active || (c0 < 0 && c1 < 0));
+    }
     uint32_t itv = 0u;   // iterations of half 0 in bits 0-15, half 1 in bits 16-31
-    if (tid < 2 * kMaxGroups) s_crc[tid] = 0u;
     uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
-    bool idle = __syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0));
     const bool run = p.max_it > 0;   // max_iterations == 0: rate recovery only, status 1
     RowMsg nxt{};
     while (!idle) {
@@ -224,17 +242,18 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
         __syncthreads();
       }
       fresh = 0u;
-      if (run) crc_pass(p, s_lq, s_crc, Bp, bpm);
+      if (run) crc_pass(p, s_lq, s_crc);
       __syncthreads();
       bool fin[2] = {false, false};
       if (active) {
         for (int h = 0; h < 2; ++h) {
-          if (cw[h] < 0) continue;
+          const int c = s_cw[2 * g + h];
+          if (c < 0) continue;
           if (run) itv += h ? 0x10000u : 1u;
           const int ith = (int)(h ? itv >> 16 : itv & 0xFFFFu);
           const bool pass = run && s_crc[2 * g + h] == 0u;
           if (pass || ith >= p.max_it) {
-            emit_block(p, lq, zx, cw[h], h, pass ? 0 : 1, ith);
+            emit_block(p, lq, zx, c, h, pass ? 0 : 1, ith);
             fin[h] = true;
           }
         }
@@ -250,18 +269,18 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
         if (fin[1]) s_cw[2 * g + 1] = nc1;
       }
       __syncthreads();
+      const int c0 = active ? s_cw[2 * g] : -1, c1 = active ? s_cw[2 * g + 1] : -1;
       if (active && (fin[0] || fin[1])) {
         for (int h = 0; h < 2; ++h) {
           if (!fin[h]) continue;
-          cw[h] = s_cw[2 * g + h];
           itv &= h ? 0x0000FFFFu : 0xFFFF0000u;
-          if (cw[h] >= 0) fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
+          if ((h ? c1 : c0) >= 0) fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
         }
-        if (!p.rr_scatter) recover_halves(p, lq, zx, cw[0], cw[1], fin[0], fin[1]);
+        if (!p.rr_scatter) recover_halves(p, lq, zx, c0, c1, fin[0], fin[1]);
       }
       // `any` is uniform here, so every thread of the CTA reaches the barriers inside
-      if (p.rr_scatter) recover_scatter(p, lq, zx, active, cw[0], cw[1], fin[0], fin[1]);
-      idle = __syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0));
+      if (p.rr_scatter) recover_scatter(p, lq, zx, active, c0, c1, fin[0], fin[1]);
+      idle = __syncthreads_and(!active || (c0 < 0 && c1 < 0));
     }
     // Every take of this CTA is done (the last barrier above).  The CTA that
     // finishes last rewinds the queue for the next launch on the stream.
@@ -325,7 +344,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
         }
 
         // ---- hard decisions + CRC of every code block in the CTA ----
-        crc_pass(p, s_lq, s_crc, Bp, bpm);
+        crc_pass(p, s_lq, s_crc);
         __syncthreads();
         bool pass0 = false, pass1 = false;
         if (active) {

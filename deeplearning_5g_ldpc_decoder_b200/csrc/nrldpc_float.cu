@@ -302,13 +302,28 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
         }
         __syncthreads();
       }
-      for (int k = tid; k < p.G * Bp; k += blockDim.x) {
-        const int gg = div_bp(k, bpm);
-        const int i = k - gg * Bp;
+      // A warp's 32 consecutive k share one slot (Bp and the block size are
+      // multiples of 32): XOR per thread, reduce once per slot.
+      {
         uint32_t r = 0u;
-        if (i < p.B && s_lqf[gg * p.lq_len + i] < 0.0f) r = crc_term(p, i);
-        r = __reduce_xor_sync(0xFFFFFFFFu, r);
-        if ((tid & 31) == 0 && r) atomicXor(&s_crc[gg], r);
+        int cur = -1;
+        for (int k = tid; k < p.G * Bp; k += blockDim.x) {
+          const int gg = div_bp(k, bpm);
+          if (gg != cur) {
+            if (cur >= 0) {
+              r = __reduce_xor_sync(0xFFFFFFFFu, r);
+              if ((tid & 31) == 0 && r) atomicXor(&s_crc[cur], r);
+            }
+            r = 0u;
+            cur = gg;
+          }
+          const int i = k - gg * Bp;
+          if (i < p.B && s_lqf[gg * p.lq_len + i] < 0.0f) r ^= crc_term(p, i);
+        }
+        if (cur >= 0) {
+          r = __reduce_xor_sync(0xFFFFFFFFu, r);
+          if ((tid & 31) == 0 && r) atomicXor(&s_crc[cur], r);
+        }
       }
       __syncthreads();
       if (active && !done && s_crc[g] == 0u) {

@@ -161,6 +161,16 @@ __device__ __noinline__ void recover_halves_mixed(const MixedParams& p, const Mi
   }
 }
 
+// XOR of the warp's partial CRC remainders of slot gg into s_crc.
+__device__ __forceinline__ void mixed_crc_flush(uint32_t* s_crc, int gg, uint32_t r0, uint32_t r1) {
+  r0 = __reduce_xor_sync(0xFFFFFFFFu, r0);
+  r1 = __reduce_xor_sync(0xFFFFFFFFu, r1);
+  if ((threadIdx.x & 31) == 0) {
+    if (r0) atomicXor(&s_crc[2 * gg], r0);
+    if (r1) atomicXor(&s_crc[2 * gg + 1], r1);
+  }
+}
+
 template <bool kDegenClip, int kThreads, int kCap, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const __grid_constant__ MixedParams p) {
   constexpr int kGroups = kCap / 2;       // G = floor(kCap / Zc) <= kCap / 2 (Zc >= 2)
@@ -247,23 +257,29 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
         __syncthreads();
       }
       fresh = 0u;
-      // Hard decisions + CRC of both halves of every group (each with its own B and CRC type).
-      for (int k = tid; run && k < G * Bp; k += blockDim.x) {
-        const int gg = div_bp(k, bpm);
-        const int i = k - gg * Bp;
-        const int4 gr = s_grp[gg];
+      // Hard decisions + CRC of both halves of every group (each with its own B
+      // and CRC type).  Bp and the block size are multiples of 32, so a warp's
+      // 32 consecutive k share one slot: terms are XORed per thread while the
+      // slot stays the same and the warp reduces once per slot.
+      {
         uint32_t r0 = 0u, r1 = 0u;
-        const uint32_t w = i < lq_len ? s_lq[gg * lq_len + i] : 0u;
-        if (i < gr.x && (w & 0x8000u) && NRLDPC_INBOUNDS(gr.x - 1 - i, kMaxB, kBoundsCrc))
-          r0 = __ldg(p.crc_tab + gr.z + (gr.x - 1 - i));
-        if (i < gr.y && (w & 0x80000000u) && NRLDPC_INBOUNDS(gr.y - 1 - i, kMaxB, kBoundsCrc))
-          r1 = __ldg(p.crc_tab + gr.w + (gr.y - 1 - i));
-        r0 = __reduce_xor_sync(0xFFFFFFFFu, r0);
-        r1 = __reduce_xor_sync(0xFFFFFFFFu, r1);
-        if ((tid & 31) == 0) {
-          if (r0) atomicXor(&s_crc[2 * gg], r0);
-          if (r1) atomicXor(&s_crc[2 * gg + 1], r1);
+        int cur = -1;
+        for (int k = tid; run && k < G * Bp; k += blockDim.x) {
+          const int gg = div_bp(k, bpm);
+          if (gg != cur) {
+            if (cur >= 0) mixed_crc_flush(s_crc, cur, r0, r1);
+            r0 = r1 = 0u;
+            cur = gg;
+          }
+          const int i = k - gg * Bp;
+          const int4 gr = s_grp[gg];
+          const uint32_t w = i < lq_len ? s_lq[gg * lq_len + i] : 0u;
+          if (i < gr.x && (w & 0x8000u) && NRLDPC_INBOUNDS(gr.x - 1 - i, kMaxB, kBoundsCrc))
+            r0 ^= __ldg(p.crc_tab + gr.z + (gr.x - 1 - i));
+          if (i < gr.y && (w & 0x80000000u) && NRLDPC_INBOUNDS(gr.y - 1 - i, kMaxB, kBoundsCrc))
+            r1 ^= __ldg(p.crc_tab + gr.w + (gr.y - 1 - i));
         }
+        if (cur >= 0) mixed_crc_flush(s_crc, cur, r0, r1);
       }
       __syncthreads();
       bool refill[2] = {false, false};
