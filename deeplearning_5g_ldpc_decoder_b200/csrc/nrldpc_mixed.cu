@@ -178,7 +178,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
   __shared__ uint32_t s_crc[2 * kGroups];
   __shared__ MixedGraph s_g;
   __shared__ int4 s_grp[kGroups];         // per group: B of both halves (0 when idle), CRC table offsets
-  __shared__ int s_cw[2 * kGroups];       // block in each half lane, -1 when idle
+  __shared__ int s_cw[2 * kGroups];       // block in each half lane, -1 when idle (not held in registers:
+                                          // the layer loop needs every register it can get)
+  __shared__ uint4 s_rows[kMaxRows];      // per-layer descriptors of the claim's graph (row_descriptor layout)
   __shared__ int s_item;
 
   const int tid = threadIdx.x;
@@ -209,50 +211,55 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
     const int zx = tid - g * Zc;
     const bool active = g < G;
     uint32_t* lq = s_lq + (active ? g : 0) * lq_len;
+    const int bi = s_g.bgn == 1 ? 0 : 1;
+    for (int r = tid; r < s_g.R; r += blockDim.x) {
+      const uint32_t e0 = s_g.row_off[r], dg = (uint32_t)s_g.row_off[r + 1] - e0;
+      const uint32_t five = s_g.lr_off[r + 1] - s_g.lr_off[r] > 4u * kThreadsTarget ? 1u : 0u;
+      s_rows[r] = make_uint4(s_g.lr_off[r], e0 | (dg << 16) | (five << 24), p.w_inline[bi][r], 0u);
+    }
     if (tid < 2 * G) s_cw[tid] = take_block(p, key);
     __syncthreads();
-    int cw[2] = {active ? s_cw[2 * g] : -1, active ? s_cw[2 * g + 1] : -1};
-    if (__syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0))) continue;   // the graph's queue is empty
-    uint32_t itv = 0u;   // iterations of half 0 in bits 0-15, half 1 in bits 16-31
-    if (active) {
-      if (zx == 0)
-        s_grp[g] = make_int4(cw[0] >= 0 ? p.cws[cw[0]].B : 0, cw[1] >= 0 ? p.cws[cw[1]].B : 0,
-                             cw[0] >= 0 ? p.cws[cw[0]].crctype * kMaxB : 0,
-                             cw[1] >= 0 ? p.cws[cw[1]].crctype * kMaxB : 0);
+    {
+      const int cw[2] = {active ? s_cw[2 * g] : -1, active ? s_cw[2 * g + 1] : -1};
+      if (__syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0))) continue;   // the graph's queue is empty
+      if (active) {
+        if (zx == 0)
+          s_grp[g] = make_int4(cw[0] >= 0 ? p.cws[cw[0]].B : 0, cw[1] >= 0 ? p.cws[cw[1]].B : 0,
+                               cw[0] >= 0 ? p.cws[cw[0]].crctype * kMaxB : 0,
+                               cw[1] >= 0 ? p.cws[cw[1]].crctype * kMaxB : 0);
+      }
+      recover_halves_mixed(p, s_g, lq, zx, active, cw, true, true);
     }
-    recover_halves_mixed(p, s_g, lq, zx, active, cw, true, true);
+    uint32_t itv = 0u;   // iterations of half 0 in bits 0-15, half 1 in bits 16-31
     if (tid < 2 * kGroups) s_crc[tid] = 0u;
     uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
     __syncthreads();
 
-    const int bi = s_g.bgn == 1 ? 0 : 1;
     const uint32_t zx4 = 4u * (uint32_t)zx;
     const uint32_t zxm4 = zx4 - 4u * (uint32_t)Zc;
     const uint32_t gb4 = 4u * (uint32_t)((active ? g : 0) * lq_len);
-    const int Bp = (s_g.K + 31) & ~31;   // every block's B <= K
-    const uint32_t bpm = bp_magic(Bp);
     RowMsg nxt{};
     for (;;) {
       const bool run = p.max_it > 0;   // max_iterations == 0: rate recovery only, status 1
       for (int row = 0; run && row < s_g.R; ++row) {
         if (active) {
           const RowMsg cur = nxt;
+          const uint4 d = s_rows[row];
           const int rn = row + 1 < s_g.R ? row + 1 : 0;
-          nxt = load_row_msg(scratch + s_g.lr_off[rn] + tid, s_g.lr_off[rn + 1] - s_g.lr_off[rn] > 4u * kThreadsTarget);
-          const int e0 = s_g.row_off[row];
-          const int deg = s_g.row_off[row + 1] - e0;
+          const uint2 dn = *reinterpret_cast<const uint2*>(&s_rows[rn]);
+          nxt = load_row_msg(scratch + dn.x + tid, row_five(dn.y));
           uint32_t ab0, ab1;
           if (p.weights_T[bi] > 0) {
             ab0 = __ldg(p.weights[bi] + (min((int)(itv & 0xFFFFu), p.weights_T[bi] - 1) * s_g.R + row));
             ab1 = __ldg(p.weights[bi] + (min((int)(itv >> 16), p.weights_T[bi] - 1) * s_g.R + row));
           } else {
-            ab0 = ab1 = p.w_inline[bi][row];
+            ab0 = ab1 = d.z;
           }
-          layer_dispatch<kDegenClip, true>(deg, p, s_g.edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
-                                           4u * (uint32_t)(G * lq_len), e0,
+          layer_dispatch<kDegenClip, true>(row_deg(d.y), p, s_g.edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
+                                           4u * (uint32_t)(G * lq_len), row_e0(d.y),
                                            (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
                                            (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, cur, fresh,
-                                           scratch + s_g.lr_off[row] + tid);
+                                           scratch + d.x + tid);
         }
         __syncthreads();
       }
@@ -262,6 +269,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
       // 32 consecutive k share one slot: terms are XORed per thread while the
       // slot stays the same and the warp reduces once per slot.
       {
+        const int Bp = (s_g.K + 31) & ~31;   // every block's B <= K
+        const uint32_t bpm = bp_magic(Bp);
         uint32_t r0 = 0u, r1 = 0u;
         int cur = -1;
         for (int k = tid; run && k < G * Bp; k += blockDim.x) {
@@ -285,12 +294,13 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
       bool refill[2] = {false, false};
       if (active) {
         for (int h = 0; h < 2; ++h) {
-          if (cw[h] < 0) continue;
+          const int c = s_cw[2 * g + h];
+          if (c < 0) continue;
           if (run) itv += h ? 0x10000u : 1u;
           const int ith = (int)(h ? itv >> 16 : itv & 0xFFFFu);
           const bool pass = run && s_crc[2 * g + h] == 0u;
           if (pass || ith >= p.max_it) {
-            mixed_emit(p, lq, zx, Zc, cw[h], h, pass ? 0 : 1, ith);
+            mixed_emit(p, lq, zx, Zc, c, h, pass ? 0 : 1, ith);
             refill[h] = true;
           }
         }
@@ -303,10 +313,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
         for (int h = 0; h < 2; ++h)
           if (refill[h]) s_cw[2 * g + h] = take_block(p, key);
       __syncthreads();
+      const int cw[2] = {active ? s_cw[2 * g] : -1, active ? s_cw[2 * g + 1] : -1};
       if (active) {
         for (int h = 0; h < 2; ++h) {
           if (!refill[h]) continue;
-          cw[h] = s_cw[2 * g + h];
           itv &= h ? 0x0000FFFFu : 0xFFFF0000u;
           if (cw[h] >= 0) fresh |= h ? 0xFFFF0000u : 0x0000FFFFu;
         }
