@@ -170,7 +170,9 @@ __device__ __forceinline__ void take_blocks(const DecodeParams& p, bool q0, bool
   }
 }
 
-template <bool kDegenClip, bool kRefill>
+// kG1: one lane pair per CTA (G = 1, Zc >= 193), so the group index and its
+// shared-memory base are compile-time zeros and free registers in the layer loop.
+template <bool kDegenClip, bool kRefill, bool kG1>
 __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __grid_constant__ DecodeParams p) {
   extern __shared__ __align__(16) uint32_t s_lq[];        // [G][lq_len] int16x2
   __shared__ uint32_t s_crc[2 * kMaxGroups];
@@ -180,9 +182,9 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
   for (int r = threadIdx.x; r < p.R; r += blockDim.x) s_rows[r] = row_descriptor(p, r);
 
   const int tid = threadIdx.x;
-  const int g = tid / p.Zc;
-  const int zx = tid - g * p.Zc;
-  const bool active = g < p.G;
+  const int g = kG1 ? 0 : tid / p.Zc;
+  const int zx = kG1 ? tid : tid - g * p.Zc;
+  const bool active = kG1 ? tid < p.Zc : g < p.G;
   uint32_t* lq = s_lq + (active ? g : 0) * p.lq_len;
   uint32_t* scratch = p.scratch + (int64_t)blockIdx.x * p.scratch_words;
   // debug build: every message word of the CTA (planes of kThreadsTarget words,
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
     return;
   const uint32_t zx4 = 4u * (uint32_t)zx;
   const uint32_t zxm4 = zx4 - 4u * (uint32_t)p.Zc;     // wraps: min(zx4+s, zxm4+s) = ((zx+V) mod Zc)*4
-  const uint32_t gb4 = 4u * (uint32_t)((active ? g : 0) * p.lq_len);
+  const uint32_t gb4 = kG1 ? 0u : 4u * (uint32_t)((active ? g : 0) * p.lq_len);
   const uint32_t lq_limit = 4u * (uint32_t)(p.G * p.lq_len);   // bytes of s_lq in use
 
   if constexpr (kRefill) {
@@ -372,20 +374,20 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
   }
 }
 
-template <bool kDegenClip, bool kRefill>
+template <bool kDegenClip, bool kRefill, bool kG1>
 int launch_fixed_t(const DecodeParams& p, int grid, int block, int smem, cudaStream_t s) {
   const cudaError_t err =
-      cudaFuncSetAttribute(fixed_pair_kernel<kDegenClip, kRefill>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      cudaFuncSetAttribute(fixed_pair_kernel<kDegenClip, kRefill, kG1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (err != cudaSuccess) return (int)err;
-  fixed_pair_kernel<kDegenClip, kRefill><<<grid, block, smem, s>>>(p);
+  fixed_pair_kernel<kDegenClip, kRefill, kG1><<<grid, block, smem, s>>>(p);
   return (int)cudaSuccess;
 }
 
 template <bool kDegenClip, bool kRefill>
 int occupancy_fixed_t(int block, int smem) {
   int n = 0;
-  cudaFuncSetAttribute(fixed_pair_kernel<kDegenClip, kRefill>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_pair_kernel<kDegenClip, kRefill>, block, smem);
+  cudaFuncSetAttribute(fixed_pair_kernel<kDegenClip, kRefill, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_pair_kernel<kDegenClip, kRefill, false>, block, smem);
   return n;
 }
 
@@ -394,10 +396,17 @@ int occupancy_fixed_t(int block, int smem) {
 int launch_fixed(const DecodeParams& p, int grid, int block, int smem, bool degen_clip, void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const bool refill = p.cursor != nullptr;
-  const int err = degen_clip ? (refill ? launch_fixed_t<true, true>(p, grid, block, smem, s)
-                                       : launch_fixed_t<true, false>(p, grid, block, smem, s))
-                             : (refill ? launch_fixed_t<false, true>(p, grid, block, smem, s)
-                                       : launch_fixed_t<false, false>(p, grid, block, smem, s));
+  const bool g1 = refill && p.G == 1;   // the queue-refill path has a one-pair specialisation
+  int err;
+  if (degen_clip) {
+    err = g1 ? launch_fixed_t<true, true, true>(p, grid, block, smem, s)
+             : (refill ? launch_fixed_t<true, true, false>(p, grid, block, smem, s)
+                       : launch_fixed_t<true, false, false>(p, grid, block, smem, s));
+  } else {
+    err = g1 ? launch_fixed_t<false, true, true>(p, grid, block, smem, s)
+             : (refill ? launch_fixed_t<false, true, false>(p, grid, block, smem, s)
+                       : launch_fixed_t<false, false, false>(p, grid, block, smem, s));
+  }
   if (err != (int)cudaSuccess) return err;
   count_launch();
   return (int)cudaGetLastError();
