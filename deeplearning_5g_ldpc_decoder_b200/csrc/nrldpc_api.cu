@@ -190,7 +190,7 @@ int trained_device_table(DeviceState* st, int bgn, const uint32_t** ptr, int* T)
 struct Plan {
   DecodeParams p;
   int grid, block, smem;
-  bool degen;
+  int clip;   // check-node arithmetic variant of the fixed-point kernel (fixed_clip_mode)
   int algo;
   size_t scratch_bytes;
 };
@@ -253,11 +253,12 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
   }
   p.rr_scatter = fixed && cp.E <= cp.Nv;
   p.qm_magic = qm_magic(cp.Qm);
+  p.one = 1u;
   p.f_alpha = (float)dc.alpha / 32768.0f;
   p.f_beta = (float)dc.beta / 128.0f;
   p.f_max = (float)dc.max_llr / 128.0f;
   p.f_min = (float)dc.min_llr / 128.0f;
-  plan->degen = dc.min_llr > dc.max_llr;
+  plan->clip = fixed_clip_mode(dc);
 
   // Scratch layout per CTA, layer by layer.
   uint32_t off = 0;
@@ -280,7 +281,7 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
 
   int occ;
   if (fixed) {
-    occ = occupancy_fixed(plan->block, plan->smem, plan->degen, true);
+    occ = occupancy_fixed(plan->block, plan->smem, plan->clip, true);
   } else if (algo == 4) {
     occ = occupancy_float_minsum(plan->block, plan->smem);
   } else {
@@ -298,7 +299,7 @@ int launch_plan(Plan* plan, void* stream) {
     case 1:
     case 2:
     case 3:
-      return launch_fixed(plan->p, plan->grid, plan->block, plan->smem, plan->degen, stream);
+      return launch_fixed(plan->p, plan->grid, plan->block, plan->smem, plan->clip, stream);
     case 4:
       return launch_float_minsum(plan->p, plan->grid, plan->block, plan->smem, stream);
     default:

@@ -172,7 +172,7 @@ __device__ __forceinline__ void take_blocks(const DecodeParams& p, bool q0, bool
 
 // kG1: one lane pair per CTA (G = 1, Zc >= 193), so the group index and its
 // shared-memory base are compile-time zeros and free registers in the layer loop.
-template <bool kDegenClip, bool kRefill, bool kG1>
+template <int kClip, bool kRefill, bool kG1>
 __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __grid_constant__ DecodeParams p) {
   extern __shared__ __align__(16) uint32_t s_lq[];        // [G][lq_len] int16x2
   __shared__ uint32_t s_crc[2 * kMaxGroups];
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
           } else {
             ab0 = ab1 = d.z;
           }
-          layer_dispatch<kDegenClip, true>(row_deg(d.y), p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
+          layer_dispatch<kClip, true, kG1>(row_deg(d.y), p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
                                            lq_limit, row_e0(d.y), (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
                                            (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, cur, fresh,
                                            scratch + d.x + tid);
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
             const uint32_t ab = p.weights_T > 0 ? __ldg(p.weights + (min(it, p.weights_T - 1) * p.R + row)) : d.z;
             const int32_t alpha = (int32_t)(int16_t)(ab & 0xFFFFu);
             const int32_t beta = ((int32_t)ab) >> 16;
-            layer_dispatch<kDegenClip, true>(row_deg(d.y), p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
+            layer_dispatch<kClip, true, kG1>(row_deg(d.y), p, s_edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
                                              lq_limit, row_e0(d.y), alpha, beta, alpha, beta, cur,
                                              it == 0 ? 0xFFFFFFFFu : 0u, scratch + d.x + tid);
           }
@@ -374,38 +374,40 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
   }
 }
 
-template <bool kDegenClip, bool kRefill, bool kG1>
+template <int kClip, bool kRefill, bool kG1>
 int launch_fixed_t(const DecodeParams& p, int grid, int block, int smem, cudaStream_t s) {
   const cudaError_t err =
-      cudaFuncSetAttribute(fixed_pair_kernel<kDegenClip, kRefill, kG1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      cudaFuncSetAttribute(fixed_pair_kernel<kClip, kRefill, kG1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (err != cudaSuccess) return (int)err;
-  fixed_pair_kernel<kDegenClip, kRefill, kG1><<<grid, block, smem, s>>>(p);
+  fixed_pair_kernel<kClip, kRefill, kG1><<<grid, block, smem, s>>>(p);
   return (int)cudaSuccess;
 }
 
-template <bool kDegenClip, bool kRefill>
+template <int kClip>
+int launch_fixed_c(const DecodeParams& p, int grid, int block, int smem, cudaStream_t s) {
+  const bool refill = p.cursor != nullptr;
+  if (refill && p.G == 1) return launch_fixed_t<kClip, true, true>(p, grid, block, smem, s);   // one-pair specialisation
+  return refill ? launch_fixed_t<kClip, true, false>(p, grid, block, smem, s)
+                : launch_fixed_t<kClip, false, false>(p, grid, block, smem, s);
+}
+
+template <int kClip, bool kRefill>
 int occupancy_fixed_t(int block, int smem) {
   int n = 0;
-  cudaFuncSetAttribute(fixed_pair_kernel<kDegenClip, kRefill, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_pair_kernel<kDegenClip, kRefill, false>, block, smem);
+  cudaFuncSetAttribute(fixed_pair_kernel<kClip, kRefill, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_pair_kernel<kClip, kRefill, false>, block, smem);
   return n;
 }
 
 }  // namespace
 
-int launch_fixed(const DecodeParams& p, int grid, int block, int smem, bool degen_clip, void* stream) {
+int launch_fixed(const DecodeParams& p, int grid, int block, int smem, int clip_mode, void* stream) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const bool refill = p.cursor != nullptr;
-  const bool g1 = refill && p.G == 1;   // the queue-refill path has a one-pair specialisation
   int err;
-  if (degen_clip) {
-    err = g1 ? launch_fixed_t<true, true, true>(p, grid, block, smem, s)
-             : (refill ? launch_fixed_t<true, true, false>(p, grid, block, smem, s)
-                       : launch_fixed_t<true, false, false>(p, grid, block, smem, s));
-  } else {
-    err = g1 ? launch_fixed_t<false, true, true>(p, grid, block, smem, s)
-             : (refill ? launch_fixed_t<false, true, false>(p, grid, block, smem, s)
-                       : launch_fixed_t<false, false, false>(p, grid, block, smem, s));
+  switch (clip_mode) {
+    case kClipDegen: err = launch_fixed_c<kClipDegen>(p, grid, block, smem, s); break;
+    case kClipOpenMax: err = launch_fixed_c<kClipOpenMax>(p, grid, block, smem, s); break;
+    default: err = launch_fixed_c<kClipClamp>(p, grid, block, smem, s); break;
   }
   if (err != (int)cudaSuccess) return err;
   count_launch();
@@ -414,9 +416,13 @@ int launch_fixed(const DecodeParams& p, int grid, int block, int smem, bool dege
 
 int bounds_read_fixed(uint32_t* out, bool reset) { return bounds_read_tu(out, reset); }
 
-int occupancy_fixed(int block, int smem, bool degen_clip, bool refill) {
-  if (degen_clip) return refill ? occupancy_fixed_t<true, true>(block, smem) : occupancy_fixed_t<true, false>(block, smem);
-  return refill ? occupancy_fixed_t<false, true>(block, smem) : occupancy_fixed_t<false, false>(block, smem);
+int occupancy_fixed(int block, int smem, int clip_mode, bool refill) {
+  switch (clip_mode) {
+    case kClipDegen: return refill ? occupancy_fixed_t<kClipDegen, true>(block, smem) : occupancy_fixed_t<kClipDegen, false>(block, smem);
+    case kClipOpenMax:
+      return refill ? occupancy_fixed_t<kClipOpenMax, true>(block, smem) : occupancy_fixed_t<kClipOpenMax, false>(block, smem);
+    default: return refill ? occupancy_fixed_t<kClipClamp, true>(block, smem) : occupancy_fixed_t<kClipClamp, false>(block, smem);
+  }
 }
 
 }  // namespace nrldpc

@@ -73,6 +73,21 @@ inline uint32_t qm_magic(int qm) {
   return qm <= 1 ? 0u : (uint32_t)((0x100000000ull + (uint64_t)qm - 1) / (uint64_t)qm);
 }
 
+// Check-node arithmetic of the fixed-point kernels (template parameter kClip):
+//  * kClipClamp: clip(rel + msg) is a clamp to [min_llr, max_llr];
+//  * kClipDegen: min_llr > max_llr, where the reference's clip is not a clamp
+//    (exact int32 arithmetic);
+//  * kClipOpenMax: max_llr = 32767, beta = 0 and one alpha per layer for every
+//    block (algos 1 and 3): the minima need no clip, the offset step is the
+//    identity, and the clamp of the new beliefs is a max with min_llr.  This is
+//    the reference's default decoder row.
+enum { kClipClamp = 0, kClipDegen = 1, kClipOpenMax = 2 };
+inline int fixed_clip_mode(const ldpc_decoder_cfg_t& dc) {
+  if (dc.min_llr > dc.max_llr) return kClipDegen;
+  if ((dc.algo == 1 || dc.algo == 3) && dc.beta == 0 && dc.max_llr == 32767) return kClipOpenMax;
+  return kClipClamp;
+}
+
 // Alpha/beta per (iteration, row): alpha in the low 16 bits, beta in the high.
 inline uint32_t pack_ab(int16_t alpha, int16_t beta) {
   return (uint32_t)(uint16_t)alpha | ((uint32_t)(uint16_t)beta << 16);
@@ -92,6 +107,7 @@ struct DecodeParams {
   int32_t rr_scatter;  // rate recovery in scatter form (E <= Nv: no LLR repeats), fixed-point kernel
   int32_t rr_vec;      // LLR rows 16-byte aligned: 8 LLRs per load in the scatter form
   uint32_t qm_magic;   // ceil(2^32 / Qm): e / Qm as __umulhi(e, qm_magic) for e < 2^16
+  uint32_t one;        // 1: an add written as a multiply-add by this launch value issues on the FMA pipe
   float f_alpha, f_beta, f_max, f_min;
   const uint32_t* weights;
   const uint32_t* crc_tab;
@@ -177,6 +193,7 @@ struct MixedParams {
   uint32_t* scratch;
   int64_t scratch_words;               // per CTA
   int32_t max_it, fill, max_llr, min_llr;
+  uint32_t one;                        // 1 (see DecodeParams::one)
   uint32_t w_inline[2][kMaxRows];      // alpha|beta<<16 per row, per base graph (algos 1, 3)
   const uint32_t* weights[2];          // algo 2 tables per base graph
   int32_t weights_T[2];
@@ -218,19 +235,18 @@ int occupancy_train(bool backward, bool f64, bool bg2, int block, int smem, bool
 // of a class holds G = floor(capacity / Zc) lane pairs per CTA.
 constexpr int kMixedClasses = 2;
 int mixed_class_capacity(int cls);
-int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream, int cls = 0);
-int prepare_mixed(bool degen_clip, int cls = 0);
-int occupancy_mixed(bool degen_clip, int cls = 0);
+int launch_mixed(const MixedParams& p, int grid, int clip_mode, void* stream, int cls = 0);
+int prepare_mixed(int clip_mode, int cls = 0);
+int occupancy_mixed(int clip_mode, int cls = 0);
 int launch_channel(const uint8_t* rm, int64_t rm_stride, int32_t num_cw, int32_t E, int32_t Qm, float nv,
                    float sigma, float A, uint64_t seed, int16_t* llr, int64_t llr_stride, float* symbols,
                    void* stream);
-int launch_fixed(const DecodeParams& p, int grid, int block, int smem, bool degen_clip,
-                 void* stream);
+int launch_fixed(const DecodeParams& p, int grid, int block, int smem, int clip_mode, void* stream);
 int launch_float_minsum(const DecodeParams& p, int grid, int block, int smem, void* stream);
 int launch_float_bp(const DecodeParams& p, int grid, int block, int smem, void* stream);
 
 // Occupancy helpers (per kernel variant).
-int occupancy_fixed(int block, int smem, bool degen_clip, bool refill = false);
+int occupancy_fixed(int block, int smem, int clip_mode, bool refill = false);
 int occupancy_float_minsum(int block, int smem);
 int occupancy_float_bp(int block, int smem);
 

@@ -171,7 +171,7 @@ __device__ __forceinline__ void mixed_crc_flush(uint32_t* s_crc, int gg, uint32_
   }
 }
 
-template <bool kDegenClip, int kThreads, int kCap, int kMinBlocks>
+template <int kClip, int kThreads, int kCap, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const __grid_constant__ MixedParams p) {
   constexpr int kGroups = kCap / 2;       // G = floor(kCap / Zc) <= kCap / 2 (Zc >= 2)
   extern __shared__ __align__(16) uint32_t s_lq[];
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
           } else {
             ab0 = ab1 = d.z;
           }
-          layer_dispatch<kDegenClip, true>(row_deg(d.y), p, s_g.edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
+          layer_dispatch<kClip, true, false>(row_deg(d.y), p, s_g.edges, reinterpret_cast<char*>(s_lq), zx4, zxm4, gb4,
                                            4u * (uint32_t)(G * lq_len), row_e0(d.y),
                                            (int32_t)(int16_t)(ab0 & 0xFFFFu), ((int32_t)ab0) >> 16,
                                            (int32_t)(int16_t)(ab1 & 0xFFFFu), ((int32_t)ab1) >> 16, cur, fresh,
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
   }
 }
 
-// Kernel instance of (degenerate clip, class).
+// Kernel instance of (check-node arithmetic variant, class).
 template <int C>
 struct MixedShape;
 template <>
@@ -343,12 +343,12 @@ struct MixedShape<1> {
   static constexpr int kThreads = 256, kCap = 240, kMinBlocks = 3;
 };
 
-template <bool D, int C>
+template <int D, int C>
 constexpr auto mixed_fn() {
   return fixed_mixed_kernel<D, MixedShape<C>::kThreads, MixedShape<C>::kCap, MixedShape<C>::kMinBlocks>;
 }
 
-template <bool D, int C>
+template <int D, int C>
 int mixed_op(int op, const MixedParams* p, int grid, cudaStream_t s, int* occ) {
   const auto fn = mixed_fn<D, C>();
   const int smem = MixedShape<C>::kCap * kMaxCols * 4;   // largest G * (N + 2Zc) words of any of its graphs
@@ -366,11 +366,18 @@ int mixed_op(int op, const MixedParams* p, int grid, cudaStream_t s, int* occ) {
   return 0;
 }
 
-int mixed_dispatch(int op, bool degen_clip, int cls, const MixedParams* p, int grid, void* stream, int* occ) {
+template <int C>
+int mixed_dispatch_c(int op, int clip_mode, const MixedParams* p, int grid, cudaStream_t s, int* occ) {
+  switch (clip_mode) {
+    case kClipDegen: return mixed_op<kClipDegen, C>(op, p, grid, s, occ);
+    case kClipOpenMax: return mixed_op<kClipOpenMax, C>(op, p, grid, s, occ);
+    default: return mixed_op<kClipClamp, C>(op, p, grid, s, occ);
+  }
+}
+
+int mixed_dispatch(int op, int clip_mode, int cls, const MixedParams* p, int grid, void* stream, int* occ) {
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (cls == 1)
-    return degen_clip ? mixed_op<true, 1>(op, p, grid, s, occ) : mixed_op<false, 1>(op, p, grid, s, occ);
-  return degen_clip ? mixed_op<true, 0>(op, p, grid, s, occ) : mixed_op<false, 0>(op, p, grid, s, occ);
+  return cls == 1 ? mixed_dispatch_c<1>(op, clip_mode, p, grid, s, occ) : mixed_dispatch_c<0>(op, clip_mode, p, grid, s, occ);
 }
 
 }  // namespace
@@ -379,15 +386,15 @@ int bounds_read_mixed(uint32_t* out, bool reset) { return bounds_read_tu(out, re
 
 int mixed_class_capacity(int cls) { return cls == 1 ? MixedShape<1>::kCap : MixedShape<0>::kCap; }
 
-int launch_mixed(const MixedParams& p, int grid, bool degen_clip, void* stream, int cls) {
-  return mixed_dispatch(1, degen_clip, cls, &p, grid, stream, nullptr);
+int launch_mixed(const MixedParams& p, int grid, int clip_mode, void* stream, int cls) {
+  return mixed_dispatch(1, clip_mode, cls, &p, grid, stream, nullptr);
 }
 
-int prepare_mixed(bool degen_clip, int cls) { return mixed_dispatch(0, degen_clip, cls, nullptr, 0, nullptr, nullptr); }
+int prepare_mixed(int clip_mode, int cls) { return mixed_dispatch(0, clip_mode, cls, nullptr, 0, nullptr, nullptr); }
 
-int occupancy_mixed(bool degen_clip, int cls) {
+int occupancy_mixed(int clip_mode, int cls) {
   int n = 0;
-  mixed_dispatch(2, degen_clip, cls, nullptr, 0, nullptr, &n);
+  mixed_dispatch(2, clip_mode, cls, nullptr, 0, nullptr, &n);
   return n;
 }
 

@@ -22,7 +22,7 @@ struct MixedPlanImpl {
   int device = 0;
   int num_cw = 0;
   int num_sms = 0;
-  bool degen = false;
+  int clip = kClipClamp;   // check-node arithmetic variant (fixed_clip_mode)
   std::vector<MixedGraph> graphs;
   std::vector<std::vector<int>> members;   // block indices per graph, in queue order
   std::vector<MixedCw> cws;
@@ -186,9 +186,9 @@ int configure(MixedPlanImpl* pl, int ctas_per_sm, int order, int cls_mode) {
     const int rc = build_items(pl);
     if (rc != NRLDPC_OK) return rc;
   }
-  int occ = occupancy_mixed(pl->degen, 0);
+  int occ = occupancy_mixed(pl->clip, 0);
   if (occ < 1) occ = 1;
-  int occ1 = occupancy_mixed(pl->degen, 1);
+  int occ1 = occupancy_mixed(pl->clip, 1);
   if (occ1 < 1) occ1 = 1;
   pl->ctas_per_sm = std::max(1, std::min(ctas_per_sm, occ));
   pl->grid_c[0] = std::max(0, std::min(pl->num_items_c[0], pl->ctas_per_sm * pl->num_sms));
@@ -226,14 +226,14 @@ int enqueue(MixedPlanImpl* pl, cudaStream_t s) {
   const bool both = pl->grid_c[0] > 0 && pl->grid_c[1] > 0;
   if (both && (cudaEventRecord(pl->fork, s) != cudaSuccess || cudaStreamWaitEvent(pl->side, pl->fork, 0) != cudaSuccess))
     return NRLDPC_ERR_CUDA;
-  if (pl->grid_c[0] > 0 && launch_mixed(pl->params, pl->grid_c[0], pl->degen, s, 0) != 0) return NRLDPC_ERR_CUDA;
+  if (pl->grid_c[0] > 0 && launch_mixed(pl->params, pl->grid_c[0], pl->clip, s, 0) != 0) return NRLDPC_ERR_CUDA;
   if (pl->grid_c[1] > 0) {
     MixedParams p1 = pl->params;
     p1.items = pl->d_items + pl->num_items_c[0];
     p1.num_items = pl->num_items_c[1];
     p1.counter = pl->params.counter + 1;
     p1.scratch = pl->d_scratch1;
-    if (launch_mixed(p1, pl->grid_c[1], pl->degen, both ? pl->side : s, 1) != 0) return NRLDPC_ERR_CUDA;
+    if (launch_mixed(p1, pl->grid_c[1], pl->clip, both ? pl->side : s, 1) != 0) return NRLDPC_ERR_CUDA;
   }
   if (both && (cudaEventRecord(pl->join, pl->side) != cudaSuccess || cudaStreamWaitEvent(s, pl->join, 0) != cudaSuccess))
     return NRLDPC_ERR_CUDA;
@@ -254,7 +254,7 @@ int execute(MixedPlanImpl* pl, const int16_t* llr, uint8_t* bits, int32_t* statu
   if (!same) {
     if (pl->exec) cudaGraphExecDestroy(pl->exec);
     pl->exec = nullptr;
-    if (prepare_mixed(pl->degen, 0) != 0 || prepare_mixed(pl->degen, 1) != 0) return NRLDPC_ERR_CUDA;
+    if (prepare_mixed(pl->clip, 0) != 0 || prepare_mixed(pl->clip, 1) != 0) return NRLDPC_ERR_CUDA;
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return NRLDPC_ERR_CUDA;
     const int rc = enqueue(pl, s);
@@ -305,7 +305,7 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
     return NRLDPC_ERR_CUDA;
   }
   pl->num_cw = num_blocks;
-  pl->degen = dc->min_llr > dc->max_llr;
+  pl->clip = fixed_clip_mode(*dc);
   std::map<std::pair<int, int>, int> gidx;
   pl->cws.resize(num_blocks);
   for (int i = 0; i < num_blocks; ++i) {
@@ -345,6 +345,7 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
   p.max_it = dc->max_iterations;
   p.fill = dc->filling_bit_value;
   p.max_llr = dc->max_llr;
+  p.one = 1u;
   p.min_llr = dc->min_llr;
   p.scratch_words = mixed_scratch_words_per_cta();
   for (int b = 0; b < 2; ++b) {

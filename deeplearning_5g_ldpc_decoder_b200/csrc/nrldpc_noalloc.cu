@@ -130,6 +130,7 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
   p.max_it = dc->max_iterations;
   p.rr_scatter = cp.E <= cp.Nv;
   p.qm_magic = qm_magic(cp.Qm);
+  p.one = 1u;
   p.harq_on = cp.harq_on;
   p.fill = dc->filling_bit_value;
   p.max_llr = dc->max_llr;
@@ -187,10 +188,10 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
             per_cta, kNoAllocScratchBytes);
     return NRLDPC_ERR_ARG;
   }
-  const bool degen = dc->min_llr > dc->max_llr;
+  const int clip = fixed_clip_mode(*dc);
   const int block = (p.nact + 31) & ~31;
   const int smem = p.G * cp.lq_len * 4;
-  int occ = occupancy_fixed(block, smem, degen);
+  int occ = occupancy_fixed(block, smem, clip);
   if (occ < 1) occ = 1;
   const int fit = (int)(kNoAllocScratchBytes / per_cta);
   const int grid = std::max(1, std::min({p.num_items, occ * nd->num_sms, fit}));
@@ -206,6 +207,6 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
   p.harq = d_harq;
   p.harq_stride = harq_stride;
   p.scratch = nd->scratch;
-  if (launch_fixed(p, grid, block, smem, degen, stream) != 0) return NRLDPC_ERR_CUDA;
+  if (launch_fixed(p, grid, block, smem, clip, stream) != 0) return NRLDPC_ERR_CUDA;
   return NRLDPC_OK;
 }

@@ -313,7 +313,7 @@ struct TbLane {
 struct TbEngine {
   int device = 0, num_sms = 0;
   int max_tbs = 0, max_cbs = 0, max_items = 0;
-  bool degen = false;
+  int clip = kClipClamp;   // check-node arithmetic variant (fixed_clip_mode)
   int grid = 1;
   MixedGraph* d_graphs = nullptr;
   const uint32_t* d_crc_tab = nullptr;
@@ -440,7 +440,7 @@ int engine_decode(TbEngine* e, int lane, const nrldpc_tb_t* d_tbs, int n, const 
   MixedParams mp = l->mp;
   mp.llr = d_llr;
   mp.harq = d_harq;
-  if (launch_mixed(mp, e->grid, e->degen, s) != 0) return NRLDPC_ERR_CUDA;
+  if (launch_mixed(mp, e->grid, e->clip, s) != 0) return NRLDPC_ERR_CUDA;
   FinishParams fp = l->fp;
   fp.out = d_out;
   fp.status = d_status;
@@ -542,7 +542,7 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
   }
   e->max_tbs = max_tbs;
   e->max_cbs = max_cbs;
-  e->degen = dc->min_llr > dc->max_llr;
+  e->clip = fixed_clip_mode(*dc);
   // graph table for every (BG, Zc) key, and the key order (more work per block first)
   std::vector<MixedGraph> graphs(kKeys);
   memset(graphs.data(), 0, graphs.size() * sizeof(MixedGraph));
@@ -560,7 +560,7 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
   std::sort(order.begin(), order.end());
   for (int r = 0; r < kKeys; ++r) e->sp.key_by_rank[r] = r < (int)order.size() ? (int16_t)order[r].second : -1;
   e->max_items = max_cbs + (int)order.size();
-  int occ = occupancy_mixed(e->degen);
+  int occ = occupancy_mixed(e->clip);
   if (occ < 1) occ = 1;
   e->grid = std::max(1, std::min(2, occ) * e->num_sms);
   bool ok = cudaMalloc(&e->d_graphs, kKeys * sizeof(MixedGraph)) == cudaSuccess &&
@@ -582,6 +582,7 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
   p.max_it = dc->max_iterations;
   p.fill = dc->filling_bit_value;
   p.max_llr = dc->max_llr;
+  p.one = 1u;
   p.min_llr = dc->min_llr;
   for (int b = 0; b < 2; ++b) {
     const BaseGraph& g = base_graph(b + 1);
@@ -599,7 +600,7 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
     engine_free(e);
     return NRLDPC_ERR_CUDA;
   }
-  if (prepare_mixed(e->degen) != 0) {
+  if (prepare_mixed(e->clip) != 0) {
     engine_free(e);
     return NRLDPC_ERR_CUDA;
   }
