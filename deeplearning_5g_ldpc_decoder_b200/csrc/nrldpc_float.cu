@@ -130,7 +130,11 @@ __device__ __forceinline__ void fms_dispatch(int deg, const DecodeParams& p, flo
 }
 
 // --------------------------------------------------------------------- BP
-__device__ __forceinline__ void prefetch_l2(const void* a) { asm volatile("prefetch.global.L2 [%0];" ::"l"(a)); }
+// cp.async.bulk.prefetch.L2: bring `bytes` (a multiple of 16, 16-byte-aligned
+// start) of global memory toward L2; a hint, nothing waits for it.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* a, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
+}
 
 __device__ __forceinline__ float bp_message(float prod) {
   // bp_message_from_product (:54-62)
@@ -295,10 +299,17 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
             // The per-edge messages of the blocks in flight exceed L2, so their
             // loads wait on DRAM: start moving the next row's (row 0 of the next
             // iteration after the last row) toward L2 while this row computes.
-            const int rn = row + 1 < p.R ? row + 1 : 0;
-            const int dn = p.row_off[rn + 1] - p.row_off[rn];
-            const uint32_t* nx = scratch + p.lr_off[rn] + tid;
-            for (int j = 0; j < dn; ++j) prefetch_l2(nx + j * NT);
+            // The row's messages are one contiguous slice of the CTA's scratch,
+            // so one thread asks for all of it with a single bulk prefetch (the
+            // 16-byte-aligned part; the slice lies inside the scratch).
+            if (tid == 0) {
+              const int rn = row + 1 < p.R ? row + 1 : 0;
+              const int dn = p.row_off[rn + 1] - p.row_off[rn];
+              const uintptr_t lo = reinterpret_cast<uintptr_t>(scratch + p.lr_off[rn]);
+              const uintptr_t hi = lo + (uintptr_t)dn * (uintptr_t)NT * 4u;
+              const uintptr_t a = (lo + 15u) & ~(uintptr_t)15u, b = hi & ~(uintptr_t)15u;
+              if (b > a) bulk_prefetch_l2(reinterpret_cast<const void*>(a), (uint32_t)(b - a));
+            }
           }
           if (kBP) {
             bp_dispatch(deg, p, lq, (uint32_t)zx, e0, it == 0, lrp, NT);
