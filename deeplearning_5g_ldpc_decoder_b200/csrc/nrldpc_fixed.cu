@@ -91,29 +91,70 @@ __device__ __forceinline__ void crc_flush(uint32_t* s_crc, int gg, uint32_t r0, 
   }
 }
 
+// All ones when the sign bit of byte b of w is set (prmt's sign-replicating
+// selector nibbles 8 | b): byte 1 holds the sign of half 0, byte 3 that of half 1.
+__device__ __forceinline__ uint32_t sign_of_byte1(uint32_t w) {
+  uint32_t r;
+  asm("prmt.b32 %0, %1, 0, 0x9999;" : "=r"(r) : "r"(w));
+  return r;
+}
+__device__ __forceinline__ uint32_t sign_of_byte3(uint32_t w) {
+  uint32_t r;
+  asm("prmt.b32 %0, %1, 0, 0xBBBB;" : "=r"(r) : "r"(w));
+  return r;
+}
+
 // Hard decisions + CRC remainder of both halves of every group into s_crc
-// (zero for a block whose CRC passes).  Bp and the block size are multiples
-// of 32, so a warp's 32 consecutive k share one slot gg and one trip count:
-// each thread XORs its terms while gg stays the same and the warp reduces
-// once per slot (once per pass when G = 1).
+// (zero for a block whose CRC passes).
+// With B a multiple of 4 each thread takes four consecutive positions per
+// step: one 16-byte shared load of their LQ words and one 16-byte load of
+// their table entries T[B-4-i0 .. B-1-i0] (16-byte aligned because B and i0
+// are multiples of 4 and each type's table starts 16-byte aligned), and per
+// position one sign mask and one three-input XOR-AND per half.  A slot spans
+// Bq = roundup(B, 128) positions, so a warp's 32 steps (128 positions) share
+// one slot and the warp reduces once per slot.  Otherwise one position per
+// step over Bp = roundup(B, 32) positions per slot.
 __device__ __forceinline__ void crc_pass(const DecodeParams& p, const uint32_t* s_lq, uint32_t* s_crc) {
-  const int Bp = (p.B + 31) & ~31;
-  const uint32_t magic = bp_magic(Bp);
   uint32_t r0 = 0u, r1 = 0u;
   int cur = -1;
-  for (int k = threadIdx.x; k < p.G * Bp; k += blockDim.x) {
-    const int gg = div_bp(k, magic);
-    if (gg != cur) {
-      if (cur >= 0) crc_flush(s_crc, cur, r0, r1);
-      r0 = r1 = 0u;
-      cur = gg;
+  if ((p.B & 3) == 0) {
+    const int Bq4 = ((p.B + 127) & ~127) >> 2;   // four-position steps per slot
+    const uint32_t magic = bp_magic(Bq4);
+    for (int k = threadIdx.x; k < p.G * Bq4; k += blockDim.x) {
+      const int gg = div_bp(k, magic);
+      if (gg != cur) {
+        if (cur >= 0) crc_flush(s_crc, cur, r0, r1);
+        r0 = r1 = 0u;
+        cur = gg;
+      }
+      const int i0 = 4 * (k - gg * Bq4);
+      if (i0 < p.B && NRLDPC_INBOUNDS(p.B - 1 - i0, kMaxB, kBoundsCrc)) {   // i0 + 4 <= B
+        const uint4 w = *reinterpret_cast<const uint4*>(s_lq + gg * p.lq_len + i0);
+        const uint4 t = __ldg(reinterpret_cast<const uint4*>(p.crc_tab + (p.B - 4 - i0)));
+        // position i0 + j pairs with T[B-1-i0-j]: t.w, t.z, t.y, t.x
+        r0 ^= (t.w & sign_of_byte1(w.x)) ^ (t.z & sign_of_byte1(w.y)) ^ (t.y & sign_of_byte1(w.z)) ^
+              (t.x & sign_of_byte1(w.w));
+        r1 ^= (t.w & sign_of_byte3(w.x)) ^ (t.z & sign_of_byte3(w.y)) ^ (t.y & sign_of_byte3(w.z)) ^
+              (t.x & sign_of_byte3(w.w));
+      }
     }
-    const int i = k - gg * Bp;
-    if (i < p.B) {
-      const uint32_t w = s_lq[gg * p.lq_len + i];
-      const uint32_t tv = crc_term(p, i);
-      r0 ^= (w & 0x8000u) ? tv : 0u;
-      r1 ^= (w & 0x80000000u) ? tv : 0u;
+  } else {
+    const int Bp = (p.B + 31) & ~31;
+    const uint32_t magic = bp_magic(Bp);
+    for (int k = threadIdx.x; k < p.G * Bp; k += blockDim.x) {
+      const int gg = div_bp(k, magic);
+      if (gg != cur) {
+        if (cur >= 0) crc_flush(s_crc, cur, r0, r1);
+        r0 = r1 = 0u;
+        cur = gg;
+      }
+      const int i = k - gg * Bp;
+      if (i < p.B) {
+        const uint32_t w = s_lq[gg * p.lq_len + i];
+        const uint32_t tv = crc_term(p, i);
+        r0 ^= tv & sign_of_byte1(w);
+        r1 ^= tv & sign_of_byte3(w);
+      }
     }
   }
   if (cur >= 0) crc_flush(s_crc, cur, r0, r1);

@@ -33,3 +33,31 @@ def test_group_index_is_exact_for_every_size():
                 assert np.array_equal(gg, k // np.uint64(bp)), (zc, cap, bp)
                 checked += 1
     assert checked > 1000
+
+
+def test_four_position_step_index_is_exact_and_aligned():
+    """The fixed-point kernel's CRC pass with B a multiple of 4: steps of four
+    positions, Bq4 = roundup(B, 128) / 4 steps per slot.  The slot index is the
+    same high multiply by ceil(2^32 / Bq4); each step's 16-byte loads start at
+    LQ word gg*lq_len + i0 and table entry B-4-i0, both multiples of 4, and stay
+    inside the block (i0 + 3 < B) and the table (B-4-i0 >= 0)."""
+    checked = 0
+    for zc in LIFTING_SIZES:
+        G = 384 // zc
+        for cols, kb in ((68, 22), (52, 10)):      # BG1, BG2: lq_len = cols*Zc, B <= K = kb*Zc
+            lq_len = cols * zc
+            assert lq_len % 4 == 0
+            for B in range(4, kb * zc + 1, 4):
+                bq4 = ((B + 127) & ~127) // 4
+                assert bq4 % 32 == 0                  # a warp's 32 steps share one slot
+                k = np.arange(G * bq4, dtype=np.uint64)
+                gg = (k * np.uint64(bp_magic(bq4))) >> np.uint64(32)
+                assert np.array_equal(gg, k // np.uint64(bq4)), (zc, B)
+                i0 = 4 * (k - gg * np.uint64(bq4))
+                live = i0 < B
+                assert np.all(i0[live] + 3 < B)
+                assert np.all((gg[live] * lq_len + i0[live]) % 4 == 0)
+                assert np.all((B - 4 - i0[live].astype(np.int64)) >= 0)
+                assert np.all((B - 4 - i0[live].astype(np.int64)) % 4 == 0)
+                checked += 1
+    assert checked > 1000
