@@ -91,19 +91,6 @@ __device__ __forceinline__ void crc_flush(uint32_t* s_crc, int gg, uint32_t r0, 
   }
 }
 
-// All ones when the sign bit of byte b of w is set (prmt's sign-replicating
-// selector nibbles 8 | b): byte 1 holds the sign of half 0, byte 3 that of half 1.
-__device__ __forceinline__ uint32_t sign_of_byte1(uint32_t w) {
-  uint32_t r;
-  asm("prmt.b32 %0, %1, 0, 0x9999;" : "=r"(r) : "r"(w));
-  return r;
-}
-__device__ __forceinline__ uint32_t sign_of_byte3(uint32_t w) {
-  uint32_t r;
-  asm("prmt.b32 %0, %1, 0, 0xBBBB;" : "=r"(r) : "r"(w));
-  return r;
-}
-
 // Hard decisions + CRC remainder of both halves of every group into s_crc
 // (zero for a block whose CRC passes).
 // With B a multiple of 4 each thread takes four consecutive positions per

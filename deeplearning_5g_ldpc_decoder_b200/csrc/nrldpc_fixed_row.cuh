@@ -26,6 +26,19 @@ __device__ __forceinline__ uint32_t sign_mask(uint32_t x) {
 template <typename P>
 __device__ __forceinline__ uint32_t add_fma(const P& p, uint32_t a, uint32_t b) { return a * p.one + b; }
 
+// Hard-decision masks: all ones when the sign bit of byte b of w is set (prmt's sign-replicating
+// selector nibbles 8 | b): byte 1 holds the sign of half 0, byte 3 that of half 1.
+__device__ __forceinline__ uint32_t sign_of_byte1(uint32_t w) {
+  uint32_t r;
+  asm("prmt.b32 %0, %1, 0, 0x9999;" : "=r"(r) : "r"(w));
+  return r;
+}
+__device__ __forceinline__ uint32_t sign_of_byte3(uint32_t w) {
+  uint32_t r;
+  asm("prmt.b32 %0, %1, 0, 0xBBBB;" : "=r"(r) : "r"(w));
+  return r;
+}
+
 // m ? a : b, bitwise.
 __device__ __forceinline__ uint32_t bsel(uint32_t m, uint32_t a, uint32_t b) { return (a & m) | (b & ~m); }
 

@@ -265,28 +265,54 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
       }
       fresh = 0u;
       // Hard decisions + CRC of both halves of every group (each with its own B
-      // and CRC type).  Bp and the block size are multiples of 32, so a warp's
-      // 32 consecutive k share one slot: terms are XORed per thread while the
-      // slot stays the same and the warp reduces once per slot.
+      // and CRC type), four positions per step: one 16-byte shared load of
+      // their LQ words and, for a half whose B is a multiple of 4 and which
+      // covers all four, one 16-byte load of its table entries
+      // T[B-4-i0 .. B-1-i0] (16-byte aligned), else one load per position.
+      // A slot spans Bq4 = roundup(K, 128) / 4 steps (every block's B <= K),
+      // a multiple of 32, so a warp's 32 steps share one slot: terms are XORed
+      // per thread while the slot stays the same and the warp reduces once per
+      // slot.
       {
-        const int Bp = (s_g.K + 31) & ~31;   // every block's B <= K
-        const uint32_t bpm = bp_magic(Bp);
+        const int Bq4 = ((s_g.K + 127) & ~127) >> 2;
+        const uint32_t bpm = bp_magic(Bq4);
         uint32_t r0 = 0u, r1 = 0u;
         int cur = -1;
-        for (int k = tid; run && k < G * Bp; k += blockDim.x) {
+        for (int k = tid; run && k < G * Bq4; k += blockDim.x) {
           const int gg = div_bp(k, bpm);
           if (gg != cur) {
             if (cur >= 0) mixed_crc_flush(s_crc, cur, r0, r1);
             r0 = r1 = 0u;
             cur = gg;
           }
-          const int i = k - gg * Bp;
+          const int i0 = 4 * (k - gg * Bq4);
           const int4 gr = s_grp[gg];
-          const uint32_t w = i < lq_len ? s_lq[gg * lq_len + i] : 0u;
-          if (i < gr.x && (w & 0x8000u) && NRLDPC_INBOUNDS(gr.x - 1 - i, kMaxB, kBoundsCrc))
-            r0 ^= __ldg(p.crc_tab + gr.z + (gr.x - 1 - i));
-          if (i < gr.y && (w & 0x80000000u) && NRLDPC_INBOUNDS(gr.y - 1 - i, kMaxB, kBoundsCrc))
-            r1 ^= __ldg(p.crc_tab + gr.w + (gr.y - 1 - i));
+          // i0 < B <= K for a half with work here, so i0 + 3 < lq_len
+          if ((i0 < gr.x || i0 < gr.y) && NRLDPC_INBOUNDS(i0 + 3, lq_len, kBoundsLq)) {
+            const uint4 w = *reinterpret_cast<const uint4*>(s_lq + gg * lq_len + i0);
+            const uint32_t wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int B = h ? gr.y : gr.x;
+              const uint32_t* tab = p.crc_tab + (h ? gr.w : gr.z);
+              uint32_t acc = 0u;
+              if (i0 + 4 <= B && (B & 3) == 0) {
+                if (NRLDPC_INBOUNDS(B - 1 - i0, kMaxB, kBoundsCrc)) {
+                  const uint4 t = __ldg(reinterpret_cast<const uint4*>(tab + (B - 4 - i0)));
+                  const uint32_t tv[4] = {t.w, t.z, t.y, t.x};   // position i0 + j pairs with T[B-1-i0-j]
+#pragma unroll
+                  for (int j = 0; j < 4; ++j) acc ^= tv[j] & (h ? sign_of_byte3(wv[j]) : sign_of_byte1(wv[j]));
+                }
+              } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                  if (i0 + j < B && NRLDPC_INBOUNDS(B - 1 - i0 - j, kMaxB, kBoundsCrc))
+                    acc ^= __ldg(tab + (B - 1 - i0 - j)) & (h ? sign_of_byte3(wv[j]) : sign_of_byte1(wv[j]));
+                }
+              }
+              if (h) r1 ^= acc; else r0 ^= acc;
+            }
+          }
         }
         if (cur >= 0) mixed_crc_flush(s_crc, cur, r0, r1);
       }

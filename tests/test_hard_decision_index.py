@@ -61,3 +61,27 @@ def test_four_position_step_index_is_exact_and_aligned():
                 assert np.all((B - 4 - i0[live].astype(np.int64)) % 4 == 0)
                 checked += 1
     assert checked > 1000
+
+
+def test_mixed_four_position_step_index_is_exact():
+    """The mixed-size kernel's CRC pass: slots of Bq4 = roundup(K, 128) / 4
+    four-position steps (every block's B <= K of its graph), G = floor(capacity
+    / Zc) slots for both CTA classes; the 16-byte LQ load of a step with work
+    (i0 < B <= K) ends inside the slot's LQ (i0 + 3 < lq_len)."""
+    checked = 0
+    for zc in LIFTING_SIZES:
+        for cap in (384, 240):
+            G = cap // zc
+            if G == 0:
+                continue
+            for cols, kb in ((68, 22), (52, 10)):
+                K, lq_len = kb * zc, cols * zc
+                bq4 = ((K + 127) & ~127) // 4
+                assert bq4 % 32 == 0
+                k = np.arange(G * bq4, dtype=np.uint64)
+                gg = (k * np.uint64(bp_magic(bq4))) >> np.uint64(32)
+                assert np.array_equal(gg, k // np.uint64(bq4)), (zc, cap, cols)
+                i0 = 4 * (k - gg * np.uint64(bq4))
+                assert np.all(i0[i0 < K] + 3 < lq_len)
+                checked += 1
+    assert checked > 150
