@@ -251,7 +251,7 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
     int e = trained_device_table(st, cp.bgn, &p.weights, &p.weights_T);
     if (e) return e;
   }
-  p.rr_scatter = fixed && cp.E <= cp.Nv;
+  p.rr_scatter = cp.E <= cp.Nv;
   p.qm_magic = qm_magic(cp.Qm);
   p.one = 1u;
   p.f_alpha = (float)dc.alpha / 32768.0f;

@@ -133,7 +133,7 @@ __device__ __forceinline__ void fms_dispatch(int deg, const DecodeParams& p, flo
 // cp.async.bulk.prefetch.L2: bring `bytes` (a multiple of 16, 16-byte-aligned
 // start) of global memory toward L2; a hint, nothing waits for it.
 __device__ __forceinline__ void bulk_prefetch_l2(const void* a, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes));
 }
 
 __device__ __forceinline__ float bp_message(float prod) {
@@ -218,6 +218,58 @@ __device__ __forceinline__ void bp_dispatch(int deg, const DecodeParams& p, floa
   }
 }
 
+// Rate recovery of the CTA's code blocks into float LQ in scatter form (E <= Nv:
+// every LLR lands on its own position), as the fixed-point kernel's
+// recover_scatter: (A) each position's LQ word holds its int32 base value
+// (filler, else the stored soft buffer with HARQ_on, else 0), (B) each LLR,
+// read with coalesced 16-byte loads where the rows allow, is added at its
+// closed-form position, (C) the sum, truncated to int16 like the reference's
+// int16 soft buffer, is stored back to the soft buffer and dequantised to
+// float (c_lib/tx_rx_process.c:42-44: exact).  Called by every thread of the
+// CTA (it holds CTA barriers); `valid` selects the threads whose group has a
+// block, `active` those that own a group.
+static __device__ void recover_scatter_f(const DecodeParams& p, float* lq, int zx, bool active, bool valid, int cw) {
+  int32_t* lqi = reinterpret_cast<int32_t*>(lq);
+  int16_t* hq = (p.harq && valid) ? p.harq + (int64_t)cw * p.harq_stride : nullptr;
+  if (active) {
+    for (int i = zx; i < p.lq_len; i += p.Zc) {
+      const bool filler = i >= p.B && i < p.K;
+      lqi[i] = !valid ? 0 : filler ? p.fill : (p.harq_on && hq) ? (int32_t)hq[i] : 0;
+    }
+  }
+  __syncthreads();
+  if (valid) {
+    const int16_t* in = p.llr + (int64_t)cw * p.llr_stride;
+    const uint32_t E = (uint32_t)p.E;
+    uint32_t e = 8u * (uint32_t)zx;
+    if (p.rr_vec) {
+      for (; e + 8u <= E; e += 8u * (uint32_t)p.Zc) {
+        const int4 v = __ldg(reinterpret_cast<const int4*>(in + e));
+        const uint32_t w4[4] = {(uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z, (uint32_t)v.w};
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int pos = scatter_position(p, e + (uint32_t)q);
+          if (NRLDPC_INBOUNDS(pos, p.lq_len, kBoundsLq)) lqi[pos] += (int32_t)(int16_t)(w4[q >> 1] >> (16 * (q & 1)));
+        }
+      }
+    }
+    for (; e < E; e += 8u * (uint32_t)p.Zc) {   // unaligned rows, and the tail of 8 LLRs
+      for (uint32_t q = e; q < e + 8u && q < E; ++q) {
+        const int pos = scatter_position(p, q);
+        if (NRLDPC_INBOUNDS(pos, p.lq_len, kBoundsLq)) lqi[pos] += (int32_t)__ldg(in + q);
+      }
+    }
+  }
+  __syncthreads();
+  if (active) {
+    for (int i = zx; i < p.lq_len; i += p.Zc) {
+      const int16_t a = (int16_t)lqi[i];
+      if (hq) hq[i] = a;
+      lq[i] = __fdiv_rn((float)a, 128.0f);
+    }
+  }
+}
+
 __device__ void emit_float_block(const DecodeParams& p, const float* lq, int zx, int cw, int status, int iters) {
   if (iters > 0 && p.bits) {
     const int nbytes = (p.B + 7) >> 3;
@@ -247,6 +299,20 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
   extern __shared__ __align__(16) float s_lqf[];     // [G][lq_len]
   __shared__ uint32_t s_crc[kMaxGroups];
   for (int e = threadIdx.x; e < kMaxNnz; e += blockDim.x) s_fedge[e] = p.edge[e];   // read after the first barrier
+  // BP: per row, the 16-byte-aligned part of the next row's message slice
+  // (row 0 of the next iteration after the last row) as {byte offset from the
+  // CTA's scratch, bytes}, for the bulk L2 prefetch in the row loop.
+  __shared__ uint2 s_pf[kMaxRows];
+  if (kBP) {
+    for (int r = threadIdx.x; r < p.R; r += blockDim.x) {
+      const int rn = r + 1 < p.R ? r + 1 : 0;
+      const uintptr_t base = reinterpret_cast<uintptr_t>(p.scratch + (int64_t)blockIdx.x * p.scratch_words);
+      const uintptr_t lo = base + 4u * (uintptr_t)p.lr_off[rn];
+      const uintptr_t hi = lo + 4u * (uintptr_t)(p.row_off[rn + 1] - p.row_off[rn]) * (uintptr_t)p.nact;
+      const uintptr_t a = (lo + 15u) & ~(uintptr_t)15u, b = hi & ~(uintptr_t)15u;
+      s_pf[r] = b > a ? make_uint2((uint32_t)(a - base), (uint32_t)(b - a)) : make_uint2(0u, 0u);
+    }
+  }
 
   const int tid = threadIdx.x;
   const int g = tid / p.Zc;
@@ -273,7 +339,8 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
     if (item >= p.num_items) break;
     const int cw = item * p.G + g;
     const bool valid = active && cw < p.num_cw;
-    if (active) {
+    if (p.rr_scatter) recover_scatter_f(p, lq, zx, active, valid, cw);
+    if (active && !p.rr_scatter) {
       const int16_t* in = p.llr + (int64_t)(valid ? cw : 0) * p.llr_stride;
       int16_t* hq = (p.harq && valid) ? p.harq + (int64_t)cw * p.harq_stride : nullptr;
       for (int i = zx; i < p.lq_len; i += p.Zc) {
@@ -303,12 +370,8 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
             // so one thread asks for all of it with a single bulk prefetch (the
             // 16-byte-aligned part; the slice lies inside the scratch).
             if (tid == 0) {
-              const int rn = row + 1 < p.R ? row + 1 : 0;
-              const int dn = p.row_off[rn + 1] - p.row_off[rn];
-              const uintptr_t lo = reinterpret_cast<uintptr_t>(scratch + p.lr_off[rn]);
-              const uintptr_t hi = lo + (uintptr_t)dn * (uintptr_t)NT * 4u;
-              const uintptr_t a = (lo + 15u) & ~(uintptr_t)15u, b = hi & ~(uintptr_t)15u;
-              if (b > a) bulk_prefetch_l2(reinterpret_cast<const void*>(a), (uint32_t)(b - a));
+              const uint2 pf = s_pf[row];
+              if (pf.y) bulk_prefetch_l2(reinterpret_cast<const char*>(scratch) + pf.x, pf.y);
             }
           }
           if (kBP) {
@@ -319,13 +382,20 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
         }
         __syncthreads();
       }
-      // A warp's 32 consecutive k share one slot (Bp and the block size are
-      // multiples of 32): XOR per thread, reduce once per slot.
+      // Hard decisions (LQ < 0) + CRC remainder per slot.  With B a multiple of
+      // 4, four positions per step (one 16-byte shared load of their beliefs,
+      // one 16-byte load of T[B-4-i0 .. B-1-i0]) over Bq4 = roundup(B, 128) / 4
+      // steps per slot; otherwise one position per step over roundup(B, 32).
+      // Either way a warp's 32 steps share one slot: XOR per thread, reduce
+      // once per slot.
       {
+        const bool quad = (p.B & 3) == 0;
+        const int span = quad ? ((p.B + 127) & ~127) >> 2 : Bp;
+        const uint32_t smag = quad ? bp_magic(span) : bpm;
         uint32_t r = 0u;
         int cur = -1;
-        for (int k = tid; k < p.G * Bp; k += blockDim.x) {
-          const int gg = div_bp(k, bpm);
+        for (int k = tid; k < p.G * span; k += blockDim.x) {
+          const int gg = div_bp(k, smag);
           if (gg != cur) {
             if (cur >= 0) {
               r = __reduce_xor_sync(0xFFFFFFFFu, r);
@@ -334,8 +404,19 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
             r = 0u;
             cur = gg;
           }
-          const int i = k - gg * Bp;
-          if (i < p.B && s_lqf[gg * p.lq_len + i] < 0.0f) r ^= crc_term(p, i);
+          if (quad) {
+            const int i0 = 4 * (k - gg * span);
+            if (i0 < p.B && NRLDPC_INBOUNDS(p.B - 1 - i0, kMaxB, kBoundsCrc)) {   // i0 + 4 <= B
+              const float4 w = *reinterpret_cast<const float4*>(s_lqf + gg * p.lq_len + i0);
+              const uint4 t = __ldg(reinterpret_cast<const uint4*>(p.crc_tab + (p.B - 4 - i0)));
+              // position i0 + j pairs with T[B-1-i0-j]
+              r ^= (w.x < 0.0f ? t.w : 0u) ^ (w.y < 0.0f ? t.z : 0u) ^ (w.z < 0.0f ? t.y : 0u) ^
+                   (w.w < 0.0f ? t.x : 0u);
+            }
+          } else {
+            const int i = k - gg * Bp;
+            if (i < p.B && s_lqf[gg * p.lq_len + i] < 0.0f) r ^= crc_term(p, i);
+          }
         }
         if (cur >= 0) {
           r = __reduce_xor_sync(0xFFFFFFFFu, r);

@@ -104,7 +104,7 @@ struct DecodeParams {
   int32_t harq_on;
   int32_t fill, max_llr, min_llr;
   int32_t weights_T;   // 0: use w_inline[row]; >0: weights[min(it,T-1)*R + row]
-  int32_t rr_scatter;  // rate recovery in scatter form (E <= Nv: no LLR repeats), fixed-point kernel
+  int32_t rr_scatter;  // rate recovery in scatter form (E <= Nv: no LLR repeats)
   int32_t rr_vec;      // LLR rows 16-byte aligned: 8 LLRs per load in the scatter form
   uint32_t qm_magic;   // ceil(2^32 / Qm): e / Qm as __umulhi(e, qm_magic) for e < 2^16
   uint32_t one;        // 1: an add written as a multiply-add by this launch value issues on the FMA pipe
