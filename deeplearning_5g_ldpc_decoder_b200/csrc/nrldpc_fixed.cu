@@ -414,7 +414,9 @@ int launch_fixed_t(const DecodeParams& p, int grid, int block, int smem, cudaStr
 template <int kClip>
 int launch_fixed_c(const DecodeParams& p, int grid, int block, int smem, cudaStream_t s) {
   const bool refill = p.cursor != nullptr;
-  if (refill && p.G == 1) return launch_fixed_t<kClip, true, true>(p, grid, block, smem, s);   // one-pair specialisation
+  if (p.G == 1)   // one-pair specialisation
+    return refill ? launch_fixed_t<kClip, true, true>(p, grid, block, smem, s)
+                  : launch_fixed_t<kClip, false, true>(p, grid, block, smem, s);
   return refill ? launch_fixed_t<kClip, true, false>(p, grid, block, smem, s)
                 : launch_fixed_t<kClip, false, false>(p, grid, block, smem, s);
 }
