@@ -53,6 +53,13 @@ __device__ __forceinline__ Real r_inf() { return (Real)INFINITY; }
 // by row; issuing the next row's lines before the current row computes hides
 // part of their DRAM latency).
 __device__ __forceinline__ void prefetch_l2(const void* a) { asm volatile("prefetch.global.L2 [%0];" ::"l"(a)); }
+// Ask L2 for the 16-byte-aligned interior of [lo, lo + bytes) with one
+// cp.async.bulk.prefetch.L2 (a hint: nothing waits for it).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* lo, size_t bytes) {
+  const uintptr_t a = (reinterpret_cast<uintptr_t>(lo) + 15u) & ~(uintptr_t)15u;
+  const uintptr_t b = (reinterpret_cast<uintptr_t>(lo) + bytes) & ~(uintptr_t)15u;
+  if (b > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(b - a)));
+}
 
 __device__ __forceinline__ uint32_t tr_addr(const TrainParams& p, int e, uint32_t zx) {
   const uint32_t ed = p.edge[e];
@@ -378,7 +385,16 @@ __global__ void __launch_bounds__(kThreadsTarget, sizeof(Real) > 4 ? 1 : 2)
       for (int row = 0; row < p.R; ++row) {
         if (valid) {
           const int e0 = p.row_off[row], deg = p.row_off[row + 1] - e0;
-          if (old_msg && row + 1 < p.R) {   // the next row's checkpointed messages (all four planes)
+          // The next row's checkpointed messages (all four planes).  Without
+          // degree-19 rows (BG2) the group's first thread asks for the code
+          // block's contiguous msg_words block with one bulk prefetch (BG2
+          // Zc64 backward 6.33 -> 6.26 ms, no spills); the BG1 instantiation,
+          // held at 80 registers, spills more with it (16.4 -> 16.9 ms) and
+          // keeps one prefetch per plane and thread.
+          if constexpr (kMaxD <= 10) {
+            if (old_msg && row + 1 < p.R && zx == 0)
+              bulk_prefetch_l2(old_msg + (size_t)(row + 1) * p.msg_words, (size_t)p.msg_words * 4u);
+          } else if (old_msg && row + 1 < p.R) {
             MsgBlock<Real> m(old_msg, row + 1, p.msg_words, p.Zc);
             prefetch_l2(m.mag + zx);
             prefetch_l2(m.mag + p.Zc + zx);
@@ -405,7 +421,16 @@ __global__ void __launch_bounds__(kThreadsTarget, sizeof(Real) > 4 ? 1 : 2)
         Real ga = 0, gb = 0;
         if (valid) {
           const int e0 = p.row_off[row], deg = p.row_off[row + 1] - e0;
-          if (row > 0) {   // tape and carry of the row back-propagated next
+          // tape and carry of the row back-propagated next (bulk, one slice
+          // each, for the BG2 instantiation as above)
+          if constexpr (kMaxD <= 10) {
+            if (row > 0 && zx == 0) {
+              const int ep = p.row_off[row - 1];
+              const size_t bytes = (size_t)(e0 - ep) * (size_t)p.Zc * sizeof(Real);
+              bulk_prefetch_l2(tape + (size_t)ep * p.Zc, bytes);
+              bulk_prefetch_l2(carry + (size_t)ep * p.Zc, bytes);
+            }
+          } else if (row > 0) {
             const int ep = p.row_off[row - 1];
             for (int j = 0; j < e0 - ep; ++j) {
               prefetch_l2(tape + (size_t)(ep + j) * p.Zc + zx);
