@@ -258,7 +258,7 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
   p.f_beta = (float)dc.beta / 128.0f;
   p.f_max = (float)dc.max_llr / 128.0f;
   p.f_min = (float)dc.min_llr / 128.0f;
-  plan->clip = fixed_clip_mode(dc);
+  plan->clip = fixed_clip_mode(dc, p.w_inline, g.rows);
 
   // Scratch layout per CTA, layer by layer.
   uint32_t off = 0;

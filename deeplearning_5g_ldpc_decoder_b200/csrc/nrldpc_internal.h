@@ -77,15 +77,19 @@ inline uint32_t qm_magic(int qm) {
 //  * kClipClamp: clip(rel + msg) is a clamp to [min_llr, max_llr];
 //  * kClipDegen: min_llr > max_llr, where the reference's clip is not a clamp
 //    (exact int32 arithmetic);
-//  * kClipOpenMax: max_llr = 32767, beta = 0 and one alpha per layer for every
-//    block (algos 1 and 3): the minima need no clip, the offset step is the
-//    identity, and the clamp of the new beliefs is a max with min_llr.  This is
-//    the reference's default decoder row.
+//  * kClipOpenMax: max_llr = 32767 and, in every layer, alpha >= 0 and
+//    beta = 0 (algos 1 and 3): the minima need no clip, the offset step is the
+//    identity, the scaled minima lie in [0, 32766], and the clamp of the new
+//    beliefs is a max with min_llr.  This is the reference's default decoder
+//    row.
+// `ab` holds each layer's packed alpha | beta << 16 as the kernels read it.
 enum { kClipClamp = 0, kClipDegen = 1, kClipOpenMax = 2 };
-inline int fixed_clip_mode(const ldpc_decoder_cfg_t& dc) {
+inline int fixed_clip_mode(const ldpc_decoder_cfg_t& dc, const uint32_t* ab, int rows) {
   if (dc.min_llr > dc.max_llr) return kClipDegen;
-  if ((dc.algo == 1 || dc.algo == 3) && dc.beta == 0 && dc.max_llr == 32767) return kClipOpenMax;
-  return kClipClamp;
+  if ((dc.algo != 1 && dc.algo != 3) || dc.max_llr != 32767) return kClipClamp;
+  for (int r = 0; r < rows; ++r)
+    if ((ab[r] >> 15) != 0u) return kClipClamp;   // alpha < 0 (bit 15) or beta != 0 (bits 16-31)
+  return kClipOpenMax;
 }
 
 // Alpha/beta per (iteration, row): alpha in the low 16 bits, beta in the high.

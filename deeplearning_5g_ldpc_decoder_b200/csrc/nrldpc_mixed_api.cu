@@ -305,7 +305,6 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
     return NRLDPC_ERR_CUDA;
   }
   pl->num_cw = num_blocks;
-  pl->clip = fixed_clip_mode(*dc);
   std::map<std::pair<int, int>, int> gidx;
   pl->cws.resize(num_blocks);
   for (int i = 0; i < num_blocks; ++i) {
@@ -360,6 +359,9 @@ int32_t nrldpc_mixed_plan_create(const nrldpc_block_t* blocks, int32_t num_block
       return NRLDPC_ERR_CUDA;
     }
   }
+  // open-max arithmetic only when both base graphs' layers qualify
+  pl->clip = fixed_clip_mode(*dc, p.w_inline[0], base_graph(1).rows);
+  if (pl->clip == kClipOpenMax) pl->clip = fixed_clip_mode(*dc, p.w_inline[1], base_graph(2).rows);
   // per-graph block queues: members of each graph in pairing order
   std::vector<int32_t> queue;
   std::vector<int32_t> base(pl->graphs.size()), count(pl->graphs.size());

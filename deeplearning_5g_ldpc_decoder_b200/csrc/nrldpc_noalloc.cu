@@ -188,7 +188,7 @@ extern "C" int32_t nrldpc_decode_batch_noalloc(const int16_t* d_llr, int64_t llr
             per_cta, kNoAllocScratchBytes);
     return NRLDPC_ERR_ARG;
   }
-  const int clip = fixed_clip_mode(*dc);
+  const int clip = fixed_clip_mode(*dc, p.w_inline, g.rows);
   const int block = (p.nact + 31) & ~31;
   const int smem = p.G * cp.lq_len * 4;
   int occ = occupancy_fixed(block, smem, clip);

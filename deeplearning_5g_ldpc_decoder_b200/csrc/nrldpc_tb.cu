@@ -542,7 +542,6 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
   }
   e->max_tbs = max_tbs;
   e->max_cbs = max_cbs;
-  e->clip = fixed_clip_mode(*dc);
   // graph table for every (BG, Zc) key, and the key order (more work per block first)
   std::vector<MixedGraph> graphs(kKeys);
   memset(graphs.data(), 0, graphs.size() * sizeof(MixedGraph));
@@ -560,7 +559,7 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
   std::sort(order.begin(), order.end());
   for (int r = 0; r < kKeys; ++r) e->sp.key_by_rank[r] = r < (int)order.size() ? (int16_t)order[r].second : -1;
   e->max_items = max_cbs + (int)order.size();
-  int occ = occupancy_mixed(e->clip);
+  int occ = occupancy_mixed(kClipClamp);   // every arithmetic variant has the same occupancy
   if (occ < 1) occ = 1;
   e->grid = std::max(1, std::min(2, occ) * e->num_sms);
   bool ok = cudaMalloc(&e->d_graphs, kKeys * sizeof(MixedGraph)) == cudaSuccess &&
@@ -596,6 +595,9 @@ int32_t nrldpc_tb_engine_create(int32_t max_tbs, int32_t max_cbs, const ldpc_dec
       return NRLDPC_ERR_CUDA;
     }
   }
+  // open-max arithmetic only when both base graphs' layers qualify
+  e->clip = fixed_clip_mode(*dc, p.w_inline[0], base_graph(1).rows);
+  if (e->clip == kClipOpenMax) e->clip = fixed_clip_mode(*dc, p.w_inline[1], base_graph(2).rows);
   if (engine_lanes(e, 1) != NRLDPC_OK) {
     engine_free(e);
     return NRLDPC_ERR_CUDA;

@@ -100,6 +100,11 @@ def test_random_llrs_saturation_and_odd_settings(oracle, cuda):
         ((2, 1000, 1, 65000, 0, 2, 0), [1, 3, 22936, 0, 1280, 32767, -32767]),    # many repetitions, int16 wrap
         ((1, 480, 3, 2400, 3, 6, 0), [4, 5, 30000, 200, -3000, 5000, -7000]),
         ((2, 1200, 1, 4000, 2, 8, 0), [0, 4, 0, 0, 1280, 20, -32768]),
+        # open-max arithmetic (max_llr 32767, beta 0) with negative alpha: scaled
+        # minima down to -32767, and alpha -32768 as int16
+        ((2, 488, 1, 1920, 0, 2, 0), [1, 6, 40000, 0, -500, 32767, -32767]),
+        ((1, 8424, 1, 25344, 0, 8, 0), [1, 4, 32768, 0, 1280, 32767, -32768]),
+        ((2, 488, 1, 1920, 1, 2, 0), [3, 6, 50000, 0, 1280, 32767, -32767]),
     ]
     for cfg, row in cases:
         E = cfg[3]
