@@ -141,6 +141,12 @@ struct DeviceState {
   std::map<cudaStream_t, Buffer> scratch;
   std::map<cudaStream_t, Buffer> queue;   // fixed point: code-block queue head + finished-CTA count
   int num_sms = 0;
+  // CTAs per SM by (kernel, clip variant, block, dynamic shared memory): the
+  // driver query costs more than a small decode's host work, so it runs once
+  std::map<uint64_t, int> occupancy;
+  // pinned staging of the single-code-block ABI: LLRs in, status and hard bits out
+  void* one_pin = nullptr;
+  size_t one_pin_bytes = 0;
 };
 
 std::map<int, DeviceState> g_dev;
@@ -279,13 +285,21 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
   p.lr_off[g.rows] = off;
   p.scratch_words = off;
 
+  const uint64_t key = ((uint64_t)(fixed ? 1 : algo == 4 ? 2 : 3) << 56) | ((uint64_t)(fixed ? plan->clip : 0) << 48) |
+                       ((uint64_t)plan->block << 32) | (uint64_t)(uint32_t)plan->smem;
   int occ;
-  if (fixed) {
-    occ = occupancy_fixed(plan->block, plan->smem, plan->clip, true);
-  } else if (algo == 4) {
-    occ = occupancy_float_minsum(plan->block, plan->smem);
+  auto hit = st->occupancy.find(key);
+  if (hit != st->occupancy.end()) {
+    occ = hit->second;
   } else {
-    occ = occupancy_float_bp(plan->block, plan->smem);
+    if (fixed) {
+      occ = occupancy_fixed(plan->block, plan->smem, plan->clip, true);
+    } else if (algo == 4) {
+      occ = occupancy_float_minsum(plan->block, plan->smem);
+    } else {
+      occ = occupancy_float_bp(plan->block, plan->smem);
+    }
+    st->occupancy[key] = occ;
   }
   if (occ < 1) occ = 1;
   plan->grid = std::min(p.num_items, occ * st->num_sms);
@@ -379,10 +393,30 @@ int32_t decode_one(int16_t* LLr, uint8_t* hardbits, ldpc_in_config_t* inconfig, 
   if (ensure(&st->one_llr, sizeof(int16_t) * std::max(cp.E, 1)) || ensure(&st->one_bits, (size_t)nbytes) ||
       ensure(&st->one_stat, 2 * sizeof(int32_t)))
     return NRLDPC_ERR_CUDA;
+  // Pinned staging [status (16 B) | hard bits | LLRs]: copies from and to the
+  // caller's pageable buffers go through it, so the device copies are plain
+  // asynchronous transfers.
+  const size_t bits_off = 16, llr_off = bits_off + (((size_t)nbytes + 15) & ~(size_t)15);
+  const size_t pin_bytes = llr_off + sizeof(int16_t) * (size_t)std::max(cp.E, 1);
+  if (st->one_pin_bytes < pin_bytes) {
+    if (st->one_pin) cudaFreeHost(st->one_pin);
+    st->one_pin = nullptr;
+    st->one_pin_bytes = 0;
+    const size_t want = std::max(pin_bytes, (size_t)(16 + 1056 + 2 * 26112));   // up to BG1 Zc=384 at E = N
+    if (cudaHostAlloc(&st->one_pin, want, cudaHostAllocDefault) != cudaSuccess) {
+      st->one_pin = nullptr;
+      return NRLDPC_ERR_CUDA;
+    }
+    st->one_pin_bytes = want;
+  }
+  char* pin = static_cast<char*>(st->one_pin);
   cudaStream_t s = st->one_stream;
-  if (cp.E > 0 &&
-      cudaMemcpyAsync(st->one_llr.ptr, LLr, sizeof(int16_t) * cp.E, cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return NRLDPC_ERR_CUDA;
+  if (cp.E > 0) {
+    memcpy(pin + llr_off, LLr, sizeof(int16_t) * cp.E);
+    if (cudaMemcpyAsync(st->one_llr.ptr, pin + llr_off, sizeof(int16_t) * cp.E, cudaMemcpyHostToDevice, s) !=
+        cudaSuccess)
+      return NRLDPC_ERR_CUDA;
+  }
   // The reference recovers into its soft buffer before it looks at algo
   // (c_lib/c_ldpc_5g_decoder.c:44-78), so an invalid algo still updates the
   // buffer: run the recovery alone (zero iterations) in that case.
@@ -397,14 +431,16 @@ int32_t decode_one(int16_t* LLr, uint8_t* hardbits, ldpc_in_config_t* inconfig, 
                                    &run, static_cast<uint8_t*>(st->one_bits.ptr), nbytes, d_stat, nullptr,
                                    nullptr, 0, st->harq, kMaxCols * kMaxZc, s);
   if (rc != NRLDPC_OK) return rc;
-  int32_t status = 1;
-  if (cudaMemcpyAsync(&status, d_stat, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+  if (cudaMemcpyAsync(pin, d_stat, sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess)
     return NRLDPC_ERR_CUDA;
   // With zero iterations the reference leaves the caller's bits untouched.
-  if (run.max_iterations > 0 && hardbits &&
-      cudaMemcpyAsync(hardbits, st->one_bits.ptr, nbytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+  const bool copy_bits = run.max_iterations > 0 && hardbits;
+  if (copy_bits && cudaMemcpyAsync(pin + bits_off, st->one_bits.ptr, nbytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
     return NRLDPC_ERR_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return NRLDPC_ERR_CUDA;
+  int32_t status = 1;
+  memcpy(&status, pin, sizeof(int32_t));
+  if (copy_bits) memcpy(hardbits, pin + bits_off, nbytes);
   if (bad_algo) {
     fprintf(stderr, "nrldpc: invalid decoding algorithm selection: %u\n", dcfg->algo);
     return NRLDPC_ERR_ALGO;

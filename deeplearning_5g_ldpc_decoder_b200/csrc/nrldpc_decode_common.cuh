@@ -4,10 +4,33 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "nrldpc_bounds.cuh"
 #include "nrldpc_internal.h"
 
 namespace nrldpc {
+
+// Largest dynamic shared memory of a decode launch: G * (N + 2Zc) words with
+// G * Zc <= 384 lifted rows, i.e. 384 * 68 words.
+constexpr int kMaxDecodeSmem = kThreadsTarget * kMaxCols * 4;
+
+// Set a decode kernel's dynamic shared-memory limit to `limit` (by default
+// kMaxDecodeSmem, at least what any of its launches asks for) once per device;
+// `done` holds one bit per device, per kernel.  The limit is never lowered, so
+// launches and occupancy queries of any size can share it, and the attribute
+// call is not paid on every launch.
+template <typename K>
+int raise_smem_limit_once(K kernel, std::atomic<uint32_t>* done, int limit = kMaxDecodeSmem) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  const uint32_t bit = dev < 32 ? 1u << dev : 0u;
+  if (bit && (done->load(std::memory_order_acquire) & bit)) return 0;
+  const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+  if (e != cudaSuccess) return (int)e;
+  if (bit) done->fetch_or(bit, std::memory_order_release);
+  return 0;
+}
 
 // Stage one code block's circular-buffer LLRs into decoder order (HARQ index).
 //

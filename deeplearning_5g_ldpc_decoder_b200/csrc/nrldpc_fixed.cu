@@ -404,9 +404,9 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __g
 
 template <int kClip, bool kRefill, bool kG1>
 int launch_fixed_t(const DecodeParams& p, int grid, int block, int smem, cudaStream_t s) {
-  const cudaError_t err =
-      cudaFuncSetAttribute(fixed_pair_kernel<kClip, kRefill, kG1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (err != cudaSuccess) return (int)err;
+  static std::atomic<uint32_t> attr_done{0};
+  const int err = raise_smem_limit_once(fixed_pair_kernel<kClip, kRefill, kG1>, &attr_done);
+  if (err != 0) return err;
   fixed_pair_kernel<kClip, kRefill, kG1><<<grid, block, smem, s>>>(p);
   return (int)cudaSuccess;
 }
@@ -424,7 +424,8 @@ int launch_fixed_c(const DecodeParams& p, int grid, int block, int smem, cudaStr
 template <int kClip, bool kRefill>
 int occupancy_fixed_t(int block, int smem) {
   int n = 0;
-  cudaFuncSetAttribute(fixed_pair_kernel<kClip, kRefill, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  static std::atomic<uint32_t> attr_done{0};
+  if (raise_smem_limit_once(fixed_pair_kernel<kClip, kRefill, false>, &attr_done) != 0) return 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fixed_pair_kernel<kClip, kRefill, false>, block, smem);
   return n;
 }

@@ -450,33 +450,36 @@ __global__ void __launch_bounds__(kThreadsTarget, 2) float_kernel(const __grid_c
 }
 
 template <typename K>
-int launch_impl(K kernel, const DecodeParams& p, int grid, int block, int smem, void* stream) {
-  cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (err != cudaSuccess) return (int)err;
+int launch_impl(K kernel, std::atomic<uint32_t>* attr_done, const DecodeParams& p, int grid, int block, int smem,
+                void* stream) {
+  const int err = raise_smem_limit_once(kernel, attr_done);
+  if (err != 0) return err;
   kernel<<<grid, block, smem, reinterpret_cast<cudaStream_t>(stream)>>>(p);
   count_launch();
   return (int)cudaGetLastError();
 }
 
 template <typename K>
-int occupancy_impl(K kernel, int block, int smem) {
+int occupancy_impl(K kernel, std::atomic<uint32_t>* attr_done, int block, int smem) {
   int n = 0;
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (raise_smem_limit_once(kernel, attr_done) != 0) return 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, smem);
   return n;
 }
 
 }  // namespace
 
+static std::atomic<uint32_t> g_attr_minsum{0}, g_attr_bp{0};   // raise_smem_limit_once, per kernel
+
 int launch_float_minsum(const DecodeParams& p, int grid, int block, int smem, void* stream) {
-  return launch_impl(float_kernel<false>, p, grid, block, smem, stream);
+  return launch_impl(float_kernel<false>, &g_attr_minsum, p, grid, block, smem, stream);
 }
 int launch_float_bp(const DecodeParams& p, int grid, int block, int smem, void* stream) {
-  return launch_impl(float_kernel<true>, p, grid, block, smem, stream);
+  return launch_impl(float_kernel<true>, &g_attr_bp, p, grid, block, smem, stream);
 }
 int bounds_read_float(uint32_t* out, bool reset) { return bounds_read_tu(out, reset); }
 
-int occupancy_float_minsum(int block, int smem) { return occupancy_impl(float_kernel<false>, block, smem); }
-int occupancy_float_bp(int block, int smem) { return occupancy_impl(float_kernel<true>, block, smem); }
+int occupancy_float_minsum(int block, int smem) { return occupancy_impl(float_kernel<false>, &g_attr_minsum, block, smem); }
+int occupancy_float_bp(int block, int smem) { return occupancy_impl(float_kernel<true>, &g_attr_bp, block, smem); }
 
 }  // namespace nrldpc

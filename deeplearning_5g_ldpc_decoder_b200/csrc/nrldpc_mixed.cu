@@ -378,8 +378,9 @@ template <int D, int C>
 int mixed_op(int op, const MixedParams* p, int grid, cudaStream_t s, int* occ) {
   const auto fn = mixed_fn<D, C>();
   const int smem = MixedShape<C>::kCap * kMaxCols * 4;   // largest G * (N + 2Zc) words of any of its graphs
-  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (err != cudaSuccess) return (int)err;
+  static std::atomic<uint32_t> attr_done{0};
+  const int err = raise_smem_limit_once(fn, &attr_done, smem);
+  if (err != 0) return err;
   if (op == 1) {
     fn<<<grid, MixedShape<C>::kThreads, smem, s>>>(*p);
     count_launch();
