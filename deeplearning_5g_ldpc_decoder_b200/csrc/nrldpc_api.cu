@@ -235,7 +235,17 @@ int make_plan(const CodeParams& cp, const ldpc_decoder_cfg_t& dc, int num_cw, De
   const int algo = dc.algo;
   plan->algo = algo;
   const bool fixed = algo == 1 || algo == 2 || algo == 3;
-  p.G = std::max(1, kThreadsTarget / cp.Zc);
+  // Groups (lane pairs, or code blocks for the float kernels) per CTA: as many
+  // as 384 threads hold, but for a small batch no more than spreading it over
+  // all SMs needs, so a few blocks do not share one SM while others idle, and a
+  // single block runs in a CTA as wide as Zc (its layer barriers wait for no
+  // idle warps).
+  {
+    const int gmax = std::max(1, kThreadsTarget / cp.Zc);
+    const int units = fixed ? (num_cw + 1) / 2 : num_cw;
+    const int spread = (units + st->num_sms - 1) / std::max(st->num_sms, 1);
+    p.G = std::max(1, std::min(gmax, spread));
+  }
   p.nact = p.G * cp.Zc;
   plan->block = (p.nact + 31) & ~31;
   plan->smem = p.G * cp.lq_len * 4;
