@@ -234,6 +234,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
     if (tid < 2 * kGroups) s_crc[tid] = 0u;
     uint32_t fresh = 0xFFFFFFFFu;   // both halves start their first iteration
     __syncthreads();
+    // A group whose two half lanes hold no block skips the row work (it only
+    // takes part in the barriers); such a group is never refilled.
+    bool busy = active && (s_cw[2 * g] >= 0 || s_cw[2 * g + 1] >= 0);
 
     const uint32_t zx4 = 4u * (uint32_t)zx;
     const uint32_t zxm4 = zx4 - 4u * (uint32_t)Zc;
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
     for (;;) {
       const bool run = p.max_it > 0;   // max_iterations == 0: rate recovery only, status 1
       for (int row = 0; run && row < s_g.R; ++row) {
-        if (active) {
+        if (busy) {
           const RowMsg cur = nxt;
           const uint4 d = s_rows[row];
           const int rn = row + 1 < s_g.R ? row + 1 : 0;
@@ -352,7 +355,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) fixed_mixed_kernel(const
                                cw[1] >= 0 ? p.cws[cw[1]].crctype * kMaxB : 0);
       }
       recover_halves_mixed(p, s_g, lq, zx, active, cw, refill[0], refill[1]);
-      if (__syncthreads_and(!active || (cw[0] < 0 && cw[1] < 0))) break;
+      busy = active && (cw[0] >= 0 || cw[1] >= 0);
+      if (__syncthreads_and(!busy)) break;
     }
   }
 }
