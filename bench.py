@@ -97,16 +97,21 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per code block of the decode kernel, from the committed ncu summary."""
+def _profile_constant(key):
+    """A figure of the committed ncu summary of the decode kernel (`key: value`)."""
     path = os.path.join(REPO, "profiles", "fixed_pair_kernel_bg1_zc384.md")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_codeword:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":")[1].split()[0])
     except OSError:
         pass
     return None
+
+
+def profiled_traffic():
+    """DRAM bytes per code block of the decode kernel, from the committed ncu summary."""
+    return _profile_constant("dram_bytes_per_codeword")
 
 
 class ClockSampler:
@@ -511,6 +516,11 @@ def run_gpu(args, rank, world, local_rank):
                                             "(profiles/fixed_pair_kernel_bg1_zc384.md) x blocks per launch"
                                             if traffic_cw else "no ncu capture of this decoder's launch"),
                          "algorithmic_bytes_per_launch": alg, "kernel_ms": round(mean_launch_ms, 4),
+                         "note": ("the algorithmic bytes count every belief and message access as HBM traffic; "
+                                  "this decoder keeps beliefs in shared memory and messages in an L2-resident "
+                                  "compressed form, so it runs above that model, and what limits it is the "
+                                  "integer ALU pipe (profile constant alu_pipe_busy)") if args.algo == 1 else None,
+                         "alu_pipe_busy": _profile_constant("alu_pipe_busy") if args.algo == 1 else None,
                          "io_bytes_per_launch": float((2 * E + (B_BITS + 7) // 8 + 4) * n_cw)},
             "iterations_executed_mean": float(np.mean(iters)),
             "converged": int(np.sum(status == 0)),

@@ -13,7 +13,8 @@
 //    both code blocks (__vsub2 / __vmaxs2 / __vibmin_u16x2 / __vadd2 ..., see
 //    nrldpc_fixed_row.cuh).
 //  * Lifted row zx of every layer is owned by one thread; a CTA holds G pairs
-//    (G = floor(384 / Zc)) so small lifting sizes still fill the CTA.
+//    (up to floor(384 / Zc); fewer when a small batch is spread over the SMs)
+//    so small lifting sizes still fill the CTA.
 //  * The beliefs LQ of all G pairs live in shared memory for the whole decode.
 //    Circulant shifts are resolved as shared-memory word addresses
 //    col*Zc + (V_ij mod Zc + zx) mod Zc.
@@ -198,7 +199,8 @@ __device__ __forceinline__ void take_blocks(const DecodeParams& p, bool q0, bool
   }
 }
 
-// kG1: one lane pair per CTA (G = 1, Zc >= 193), so the group index and its
+// kG1: one lane pair per CTA (G = 1: Zc >= 193, or a batch small enough to
+// give every pair its own CTA), so the group index and its
 // shared-memory base are compile-time zeros and free registers in the layer loop.
 template <int kClip, bool kRefill, bool kG1>
 __global__ void __launch_bounds__(kThreadsTarget, 2) fixed_pair_kernel(const __grid_constant__ DecodeParams p) {

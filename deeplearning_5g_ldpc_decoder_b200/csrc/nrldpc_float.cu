@@ -10,7 +10,7 @@
 // the C reference to a tolerance.  Evaluating them in double precision instead
 // (nearly always the correctly rounded float) costs 3x the decode time.
 //
-// Mapping: one code block per group of Zc threads, G = floor(384 / Zc) groups
+// Mapping: one code block per group of Zc threads, up to G = floor(384 / Zc) groups
 // per CTA, FP32 beliefs in shared memory, persistent grid.  Min-sum messages
 // are stored compressed per lifted check row (two minima, flip bits, the
 // minimum's position: 16 bytes); BP messages are stored per edge.
