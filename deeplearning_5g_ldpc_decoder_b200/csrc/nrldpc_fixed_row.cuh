@@ -247,7 +247,10 @@ __device__ __forceinline__ void row_update(const P& p, const uint2* __restrict__
         sum = __vadd2(__vadd2(rel[j], t), mf & 0x00010001u);
         ovf |= (sum ^ rel[j]) & ~(rel[j] ^ mf);
       } else {
-        // any int16 scaled minimum (v = -32768 negated stays -32768)
+        // Scaled minima may be negative here (a negative alpha): neither mf
+        // (an unflipped v < 0) nor t (a flipped v = -32768, which stays
+        // -32768) always has lr's sign, so test lr itself
+        // (tests/test_row_arithmetic_identities.py).
         const uint32_t lr = __vadd2(t, mf & 0x00010001u);
         sum = __vadd2(rel[j], lr);
         ovf |= (sum ^ rel[j]) & ~(rel[j] ^ lr);
